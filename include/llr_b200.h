@@ -1,0 +1,235 @@
+/*
+ * llr_b200.h -- C ABI of the B200-native LLR diffusion-MRI reconstruction hot path.
+ *
+ * Conventions (same as wyatt-A/llr-reco):
+ *   - volumes are (nx, ny, nz, nq) complex64, column-major, x fastest, volume index
+ *     last (src/array_utils.rs:4-17);
+ *   - Casorati batches are (m, n, batch) column-major (src/block.rs:147-164);
+ *   - llr_cf32 is layout-identical to Rust's Complex32 and CUDA's cuComplex.
+ * Every entry point returns an int status (LLR_OK == 0, negative on error) and never
+ * aborts; llr_last_error() gives the message of the calling thread's last failure.
+ * "_dev" entry points take device pointers and a cudaStream_t (passed as void*, NULL =
+ * legacy default stream); host-slice entry points take host pointers and block.
+ */
+#ifndef LLR_B200_H
+#define LLR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct { float re, im; } llr_cf32;
+typedef struct llr_ctx llr_ctx;
+
+enum llr_status {
+  LLR_OK = 0,
+  LLR_ERR_INVALID = -1,     /* bad argument or configuration                     */
+  LLR_ERR_CUDA = -2,        /* CUDA runtime error                                */
+  LLR_ERR_CUFFT = -3,       /* cuFFT error                                        */
+  LLR_ERR_NOMEM = -4,       /* device or host allocation failed                  */
+  LLR_ERR_NOT_FINITE = -5,  /* non-finite objective detected                      */
+  LLR_ERR_STATE = -6,       /* call out of order (e.g. iterate before upload)    */
+  LLR_ERR_UNSUPPORTED = -7, /* shape outside what the kernels support            */
+  LLR_ERR_NO_DEVICE = -8    /* no CUDA device                                    */
+};
+
+enum llr_prox_mode {
+  LLR_PROX_HARD_RANK = 0,   /* keep the top `rank` singular triplets (low_rank.rs:10-69) */
+  LLR_PROX_SOFT_THRESH = 1  /* singular values s -> max(s - lambda, 0)                   */
+};
+
+enum llr_direction { LLR_FORWARD = 0, LLR_INVERSE = 1 }; /* signal_model.rs:13-17 */
+
+/* Recon parameters: mirrors LlrReconParams (src/lib.rs:47-81) plus the B200 build's
+ * additions (prox mode, absolute threshold, wavelet choice, seed). */
+typedef struct llr_config {
+  int32_t vol_size[3];        /* nx, ny, nz                                          */
+  int32_t nq;                 /* number of volumes                                   */
+  int32_t block_size[3];      /* llr_block_size (default 32^3)                       */
+  int32_t max_rand_shift[3];  /* 0 -> volume size (lib.rs:260)                       */
+  int32_t prox_mode;          /* enum llr_prox_mode (default HARD_RANK)              */
+  int32_t rank;               /* llr_block_rank (default 6)                          */
+  float lambda;               /* absolute singular-value threshold for SOFT_THRESH   */
+  float wavelet_alpha;        /* wavelet_shrink_factor; 0 disables the wavelet step  */
+  int32_t wavelet_moments;    /* Daubechies order: 2 (reference) or 4                */
+  int32_t wavelet_levels;     /* 0 -> maximum level (lib.rs:441)                     */
+  int32_t subspace_rank;      /* 0 -> no subspace; else nq x srank matrix uploaded   */
+  int32_t fft_max_batch_size; /* accepted for compatibility (lib.rs:54); unused      */
+  int32_t cas_mat_max_batch_size; /* accepted for compatibility (lib.rs:56); unused  */
+  int32_t n_iter;             /* default iteration count (lib.rs:62)                 */
+  uint64_t seed;              /* key of the counter-based shift RNG                  */
+  int32_t device;             /* CUDA device ordinal                                 */
+  int32_t reserved[7];
+} llr_config;
+
+/* ---- library / errors ------------------------------------------------------------ */
+const char* llr_version(void);
+const char* llr_last_error(void);
+const char* llr_status_string(int status);
+/* LlrReconParams::default() (lib.rs:67-81). */
+int llr_config_default(llr_config* cfg);
+/* Host-side validation of a configuration (no device access). */
+int llr_config_validate(const llr_config* cfg);
+
+/* ---- counter-based RNG, shapes and masks (host, no device access) ----------------- */
+/* rand_shift (lib.rs:420-427), keyed by (seed, iteration): out[a] in [0, max_shift[a]). */
+int llr_rand_shift(uint64_t seed, int64_t iteration, const int32_t max_shift[3], int32_t out[3]);
+/* grid_dim (block.rs:112-118). */
+int llr_grid_dim(const int32_t vol_size[3], const int32_t block_size[3], int32_t out[3]);
+/* Variable-density ky-kz sampling mask, uint8 (ny, nz, nq), bit-exact with the oracle. */
+int llr_vd_mask(int32_t ny, int32_t nz, int32_t nq, double accel, int32_t centre,
+                uint64_t seed, uint8_t* out);
+/* Orthogonal Daubechies filters (order 1..10): lo_d, hi_d, lo_r, hi_r of 2*order taps
+ * (the bank the dwt crate supplies at cudwt3.rs:27-31). */
+int llr_daubechies_filters(int32_t order, float* lo_d, float* hi_d, float* lo_r, float* hi_r);
+
+/* ---- context: device-resident reconstruction -------------------------------------- */
+int llr_ctx_create(const llr_config* cfg, llr_ctx** out);
+int llr_ctx_destroy(llr_ctx* ctx);
+int llr_ctx_set_stream(llr_ctx* ctx, void* stream);
+int llr_ctx_get_config(const llr_ctx* ctx, llr_config* out);
+/* Measurements y (host, (nx,ny,nz,nq)); the data-consistency set is {y != 0}
+ * (lib.rs:392-406).  Line-structured sets (whole x-lines, data_import.rs:416-438) take
+ * the hybrid-space fast path; any other pattern takes the element-wise path. */
+int llr_upload_kspace(llr_ctx* ctx, const llr_cf32* y);
+/* Same, from a device buffer in reference layout (left unmodified). */
+int llr_upload_kspace_dev(llr_ctx* ctx, const llr_cf32* d_y);
+/* Linear phase corrections, nq x 3 floats each (signal_model.rs:28-33); NULL = zeros.
+ * Must precede llr_upload_kspace. */
+int llr_set_linear_corrections(llr_ctx* ctx, const float* lin_ksp, const float* lin_img);
+/* estimate_linear_correction (signal_model.rs:100-106) for every volume of y (host). */
+int llr_estimate_linear_corrections(const llr_cf32* y, const int32_t vol_size[3], int32_t nq,
+                                    float* lin_ksp_out);
+/* Subspace matrix S, nq x srank column-major (lib.rs:210-219). */
+int llr_upload_subspace(llr_ctx* ctx, const llr_cf32* S);
+/* Set the iterate to the zero-filled image A^H y (lib.rs:233-242). */
+int llr_init_zero_filled(llr_ctx* ctx);
+int llr_upload_image(llr_ctx* ctx, const llr_cf32* x);
+int llr_upload_image_dev(llr_ctx* ctx, const llr_cf32* d_x);
+int llr_download_image(llr_ctx* ctx, llr_cf32* x);
+int llr_download_image_dev(llr_ctx* ctx, llr_cf32* d_x);
+/* Run n iterations of lib.rs:262-341 (LLR -> wavelet -> A -> hard DC -> A^H) as one
+ * CUDA graph per iteration.  resid_hist (host, may be NULL) receives the per-iteration
+ * sum of squared data-consistency errors (f64). */
+int llr_iterate(llr_ctx* ctx, int32_t n_iter, double* resid_hist);
+/* Enqueue n iterations on the context stream without synchronising (no history copy). */
+int llr_iterate_async(llr_ctx* ctx, int32_t n_iter);
+int llr_get_iteration(const llr_ctx* ctx, int64_t* it);
+int llr_set_iteration(llr_ctx* ctx, int64_t it);
+/* Residual history of the last `count` iterations ending at the current one. */
+int llr_get_residual_history(llr_ctx* ctx, double* out, int32_t count);
+/* sum |y|^2 and numel/nnz of the measurements (lib.rs:409-417). */
+int llr_measurement_stats(llr_ctx* ctx, double* total_energy, double* undersampling);
+/* Largest block singular value of the current iterate at `shift` (FP32 Gram + Jacobi). */
+int llr_sigma_max(llr_ctx* ctx, const int32_t shift[3], double* sigma_max);
+int llr_set_lambda(llr_ctx* ctx, float lambda);
+/* Single operator steps on the context iterate (for tests and custom loops). */
+int llr_ctx_prox_llr(llr_ctx* ctx, const int32_t shift[3]);
+int llr_ctx_wavelet(llr_ctx* ctx);
+int llr_ctx_data_consistency(llr_ctx* ctx, double* resid);
+/* Bytes of device memory held by the context. */
+int llr_ctx_device_bytes(const llr_ctx* ctx, size_t* bytes);
+
+/* ---- device-pointer operators (reference layout) ---------------------------------- */
+/* signal_model (signal_model.rs:34-79): in place on d_x (nx,ny,nz,batch). lin_* are
+ * host arrays of batch x 3 floats (NULL = zeros). */
+int llr_signal_model_dev(llr_cf32* d_x, const int32_t image_size[3], int32_t batch,
+                         const float* lin_ksp, const float* lin_img, int32_t direction,
+                         void* stream);
+/* lift_data_set / un_lift_data_set (block.rs:147-184) on device buffers. */
+int llr_lift_data_set_dev(const llr_cf32* d_vol, int32_t nq, llr_cf32* d_mat,
+                          const int32_t vol_size[3], const int32_t block_size[3],
+                          const int32_t shift[3], int64_t start, int64_t n, void* stream);
+int llr_un_lift_data_set_dev(llr_cf32* d_vol, int32_t nq, const llr_cf32* d_mat,
+                             const int32_t vol_size[3], const int32_t block_size[3],
+                             const int32_t shift[3], int64_t start, int64_t n, void* stream);
+/* cu_low_rank_approx_batch (low_rank.rs:10-69) in place on (m, n, batch), n <= 64. */
+int llr_low_rank_batch_dev(int32_t m, int32_t n, int32_t rank, int32_t batch,
+                           llr_cf32* d_mats, void* stream);
+/* Singular-value soft threshold of every (m, n) matrix, n <= 64. */
+int llr_soft_threshold_batch_dev(int32_t m, int32_t n, float lambda, int32_t batch,
+                                 llr_cf32* d_mats, void* stream);
+/* LR(X S) S^H per Casorati matrix (lib.rs:281-289, dti_subspace.rs:141-221). */
+int llr_subspace_low_rank_batch_dev(int32_t m, int32_t nq, int32_t srank, int32_t prox_mode,
+                                    int32_t rank, float lambda, const llr_cf32* d_S,
+                                    int32_t batch, llr_cf32* d_mats, void* stream);
+/* rhsCdgmmBatched (kernels.cu:49-67): A[:, j, b] *= d[j, b]. Returns a cudaError_t. */
+int rhsCdgmmBatched(int m, int n, int batch_size, llr_cf32* d_matrix, float* d_diag);
+/* cublas_cgemm_strided_batched_device (cublas.rs:12-105) semantics, own kernel. */
+int llr_cgemm_strided_batched_dev(int32_t m, int32_t k, int32_t n, int32_t batch,
+                                  int32_t broadcast_a, llr_cf32 alpha, llr_cf32 beta,
+                                  int32_t transpose_a, int32_t transpose_b,
+                                  const llr_cf32* d_a, const llr_cf32* d_b, llr_cf32* d_c,
+                                  void* stream);
+/* dwt3_axis / idwt3_axis (kernels.cu:273-348): one-level analysis / synthesis along
+ * `axis`; sizes and shift are HOST arrays; filters are device arrays.  The circular
+ * shift wraps each axis by its own extent (kernels.cu:80-95 wraps all by vol_size[0]). */
+int llr_dwt3_axis_dev(const llr_cf32* d_vol, llr_cf32* d_decomp, const uint32_t vol_size[3],
+                      const uint32_t decomp_size[3], uint32_t axis, uint32_t filter_len,
+                      const float* d_lo_d, const float* d_hi_d, const int32_t shift[3],
+                      void* stream);
+int llr_idwt3_axis_dev(llr_cf32* d_vol, const llr_cf32* d_decomp, const uint32_t vol_size[3],
+                       const uint32_t decomp_size[3], uint32_t axis, uint32_t filter_len,
+                       const float* d_lo_r, const float* d_hi_r, const int32_t shift[3],
+                       void* stream);
+/* wavelet_denoise (lib.rs:430-458) on nvol volumes in place; levels 0 -> max. */
+int llr_wavelet_denoise_dev(llr_cf32* d_vols, const int32_t vol_size[3], int32_t nvol,
+                            int32_t moments, int32_t levels, float alpha, void* stream);
+/* hard_project (lib.rs:392-406): where y != 0, accumulate |x - y|^2 (f64) and x := y. */
+int llr_hard_project_dev(llr_cf32* d_x, const llr_cf32* d_y, int64_t n, double* sum_sq_error,
+                         void* stream);
+
+/* ---- host-slice entry points with the reference's argument order ------------------ */
+/* cu_low_rank_approx_batch(m, n, rank, batch_size, &mut [Complex32]) (low_rank.rs:10). */
+int llr_cu_low_rank_approx_batch(size_t m, size_t n, size_t rank, size_t batch_size,
+                                 llr_cf32* matrix_data);
+/* signal_model(x, image_size, batch_size, lin_ksp_corr, lin_img_corr, direction)
+ * (signal_model.rs:34). */
+int llr_signal_model(llr_cf32* x, const size_t image_size[3], size_t batch_size,
+                     const float* lin_ksp_corr, const float* lin_img_corr, int32_t direction);
+/* lift_data_set(volumes, matrix_data, vol_size, block_size, shift, start, n)
+ * (block.rs:147); volumes is nvols contiguous volumes. */
+int llr_lift_data_set(const llr_cf32* volumes, size_t nvols, llr_cf32* matrix_data,
+                      const size_t vol_size[3], const size_t block_size[3],
+                      const size_t shift[3], size_t matrix_idx_start, size_t n_matrices);
+int llr_un_lift_data_set(llr_cf32* volumes, size_t nvols, const llr_cf32* matrix_data,
+                         const size_t vol_size[3], const size_t block_size[3],
+                         const size_t shift[3], size_t matrix_idx_start, size_t n_matrices);
+/* dti_project / dti_back_project (dti_subspace.rs:141,172). */
+int llr_dti_project(const llr_cf32* subspace_matrix, const llr_cf32* image_matrices,
+                    llr_cf32* compressed_matrices, size_t batch_size, size_t nq, size_t nvox,
+                    size_t srank);
+int llr_dti_back_project(const llr_cf32* subspace_matrix, llr_cf32* image_matrices,
+                         const llr_cf32* compressed_matrices, size_t batch_size, size_t nq,
+                         size_t nvox, size_t srank);
+/* cu_dwt_denoise(vol, vol_size, lo_d, hi_d, lo_r, hi_r, rand_shift) (cudwt3.rs:102):
+ * one-level 3-axis analysis followed by synthesis (no shrinkage). */
+int llr_cu_dwt_denoise(llr_cf32* vol_data, const size_t vol_size[3], const float* lo_d,
+                       const float* hi_d, const float* lo_r, const float* hi_r,
+                       size_t filter_len, const int32_t rand_shift[3]);
+
+/* ---- pinned host memory helpers (for end-to-end callers) -------------------------- */
+int llr_host_alloc(size_t bytes, void** out);
+int llr_host_free(void* p);
+int llr_device_alloc(size_t bytes, void** out);
+int llr_device_free(void* p);
+int llr_memcpy_h2d(void* dst, const void* src, size_t bytes, void* stream);
+int llr_memcpy_d2h(void* dst, const void* src, size_t bytes, void* stream);
+int llr_stream_sync(void* stream);
+int llr_device_count(int32_t* n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+#endif /* LLR_B200_H */

@@ -1,0 +1,139 @@
+// Internal declarations shared by the library translation units.
+#pragma once
+
+#include <cufft.h>
+#include <vector>
+#include <mutex>
+
+#include "llr_common.cuh"
+
+namespace llr {
+
+constexpr int kLlrThreads = 256;
+
+// Where the Casorati matrices of one prox launch come from and go to.
+struct BlockSource {
+  int kind;            // 0: contiguous (m, n, batch) matrices; 1: planar volume blocks
+  float2* data;
+  long long nblocks;
+  // kind 1 only
+  Geom g;
+  int bx, by, bz;      // block size
+  int gx, gy, gz;      // blocks per axis
+  int sx, sy, sz;      // explicit shift (used when it_ptr == nullptr)
+  const long long* it_ptr;  // device iteration counter; shift drawn on device when set
+  unsigned long long seed;
+  int mx, my, mz;      // max random shift per axis
+  float load_scale;    // value = raw * load_scale * conj(phase)
+  PhaseTab ph;         // phase tables (null members: identity)
+  int store_phase;     // 1: stored value = value * phase; 0: stored value = value
+  float store_scale;   // stored value additionally scaled by this factor
+};
+
+struct ProxOp {
+  int m, n;
+  int mode;            // LLR_PROX_HARD_RANK / LLR_PROX_SOFT_THRESH
+  int rank;
+  float lambda;
+  float* block_stat;   // when non-null: write the largest Gram eigenvalue, skip the update
+};
+
+int launch_llr_prox(const BlockSource& src, const ProxOp& op, cudaStream_t stream);
+bool llr_prox_supported(int m, int n);
+
+struct SubspaceOp {
+  int m, nq, srank;
+  int mode, rank;
+  float lambda;
+  const float2* S;     // nq x srank column-major
+};
+int launch_llr_prox_subspace(const BlockSource& src, const SubspaceOp& op, cudaStream_t stream);
+
+// layout / transform kernels (signal_model.cu)
+int launch_ref_to_planar(const float2* ref, float2* planar, const Geom& g, float scale, PhaseTab ph,
+                         int phase_sign, cudaStream_t s);
+int launch_planar_to_ref(const float2* planar, float2* ref, const Geom& g, float scale, PhaseTab ph,
+                         int phase_sign, cudaStream_t s);
+int launch_scale_uncovered(float2* data, const Geom& g, const int* grid_cover, const long long* it_ptr,
+                           unsigned long long seed, const int shift[3], const int maxs[3], float scale,
+                           PhaseTab ph, int conj_phase, cudaStream_t s);
+
+// wavelet (wavelet.cu)
+struct WaveletPlan {
+  int nx, ny, nz;      // volume size (in the storage axis order used by the caller)
+  int levels;
+  int flen;
+  float lo_d[20], hi_d[20], lo_r[20], hi_r[20];
+  std::vector<int> sizes;   // per level l: input extents (3 ints) ; level count + 1 entries
+};
+int wavelet_plan_init(WaveletPlan* p, int nx, int ny, int nz, int moments, int levels);
+size_t wavelet_workspace_elems(const WaveletPlan& p, int nvol);
+// Denoise nvol volumes stored with element (ix,iy,iz,v) at ix*sx + iy*sy + iz*sz + v*sv.
+int wavelet_denoise_strided(const WaveletPlan& p, float2* data, long long sx, long long sy, long long sz,
+                            long long sv, int nvol, float alpha, float2* work, cudaStream_t s);
+
+// plan cache for stand-alone signal-model calls
+int get_c2c_plan(int rank, const long long* n, long long batch, cufftHandle* out);
+int cufft_error(cufftResult r, const char* what);
+
+}  // namespace llr
+
+// -------------------------------------------------------------------------------------
+// context
+// -------------------------------------------------------------------------------------
+struct llr_ctx {
+  llr_config cfg;
+  int device;
+  cudaStream_t stream;
+  bool own_stream;
+  Geom g;
+  int m;                    // voxels per block
+  int gx, gy, gz;           // block grid
+  long long nblocks;
+  // state
+  bool have_kspace;
+  bool have_image;
+  bool hybrid;              // line-structured measurements: x-transform eliminated
+  float load_scale;         // 1 / N_t
+  // device buffers
+  float2* d_x;              // iterate (planar, raw convention)
+  float2* d_work;           // E-sized scratch
+  float2* d_yhat;           // hybrid: compact sampled lines; general: full planar
+  int* d_samp_pos;          // hybrid: sampled (ky + ny*kz) per volume, concatenated
+  long long* d_samp_off;    // hybrid: nq + 1 offsets into d_samp_pos
+  std::vector<long long> h_samp_off;
+  long long n_samp_lines;
+  float2* d_ph_ksp;         // (nx + ny + nz) * nq  image-domain phase  e^{+i theta_ksp}
+  float2* d_ph_img;         // (nx + ny + nz) * nq  k-domain phase      e^{+i theta_img}
+  float2* d_S;              // subspace (nq x srank)
+  double* d_partials;
+  int n_partials;
+  double* d_hist;
+  long long hist_cap;
+  long long* d_iter;
+  long long h_iter;         // host mirror (valid after sync)
+  float* d_block_stat;
+  float2* d_wavelet_work;
+  size_t wavelet_work_elems;
+  llr::WaveletPlan wplan;
+  bool wavelet_on;
+  // FFT
+  cufftHandle plan_fwd;     // hybrid: 2-D over (z, y) per plane; general: 3-D
+  bool have_plan;
+  void* d_fft_work;
+  size_t fft_work_bytes;
+  // graph
+  cudaGraph_t graph;
+  cudaGraphExec_t graph_exec;
+  bool have_graph;
+  // measurement stats
+  double total_energy;
+  double undersampling;
+  std::vector<float> lin_ksp, lin_img;   // nq * 3
+};
+
+namespace llr {
+int ctx_enqueue_iteration(llr_ctx* ctx, cudaStream_t s);
+int ctx_prox(llr_ctx* ctx, cudaStream_t s, const int* explicit_shift, float* block_stat);
+PhaseTab ctx_phase(const llr_ctx* ctx, const float2* base, bool with_x);
+}

@@ -1,0 +1,212 @@
+"""GPU parity of the device-resident reconstruction (C-ABI context) against the FP64 oracle.
+
+Every case runs the same seeded phantom through ``llr_iterate`` (CUDA graph replay, shifts
+drawn on the device) and through ``oracle.recon`` with the same counter-based shift
+sequence.  Tolerance: relative L2 error of the image <= 2e-4 (complex FP32 vs FP64) and of
+each per-iteration data-consistency residual <= 2e-4.
+"""
+import numpy as np
+import pytest
+
+from conftest import crandn, rel_err
+from oracle import llr_oracle as O
+
+import llr_b200
+from llr_b200 import ReconContext, ReconParams, _lib as L
+from llr_b200.phantom import dti_subspace, make_dataset
+
+pytestmark = pytest.mark.gpu
+
+TOL = 2e-4
+
+
+def dataset(vol, nq, accel=3.0, seed=0, centre=6):
+    shells = [(0, 1), (1000, nq - 1)]
+    return make_dataset(vol, shells, accel, seed, centre=centre, mask_fn=O.vd_mask)
+
+
+def oracle_cfg(bs, mode, rank=0, lam=0.0, seed=0, **kw):
+    return O.ReconConfig(block_size=tuple(bs), mode=mode, rank=rank, lam=lam, seed=seed, **kw)
+
+
+def run_both(y, bs, mode, n_iter, rank=2, lam_rel=0.02, seed=5, lin=None, wavelet=None, subspace=None,
+             max_shift=None):
+    nx, ny, nz, nq = y.shape
+    ocfg = oracle_cfg(bs, "hard" if mode == L.LLR_PROX_HARD_RANK else "soft", rank=rank, seed=seed,
+                      max_rand_shift=max_shift)
+    if lin is not None:
+        ocfg.lin_ksp, ocfg.lin_img = lin
+    if subspace is not None:
+        ocfg.subspace = subspace.astype(np.complex128)
+    x0 = O.zero_filled(y.astype(np.complex128), ocfg)
+    lam = 0.0
+    if mode == L.LLR_PROX_SOFT_THRESH:
+        lam = lam_rel * O.sigma_max(x0, bs)
+        ocfg.lam = lam
+    if wavelet is not None:
+        ocfg.wavelet_alpha, ocfg.wavelet_moments, ocfg.wavelet_levels = wavelet
+    p = ReconParams(vol_size=(nx, ny, nz), nq=nq, block_size=bs, prox_mode=mode, rank=rank, lam=lam, seed=seed,
+                    max_rand_shift=max_shift,
+                    subspace_rank=0 if subspace is None else subspace.shape[1])
+    if wavelet is not None:
+        p.wavelet_alpha, p.wavelet_moments, p.wavelet_levels = wavelet
+    with ReconContext(p) as ctx:
+        if lin is not None:
+            ctx.set_linear_corrections(lin[0], lin[1])
+        ctx.upload_kspace(y)
+        if subspace is not None:
+            ctx.upload_subspace(subspace)
+        ctx.init_zero_filled()
+        g0 = ctx.download_image()
+        assert rel_err(g0, x0) < 2e-6, "zero-filled image"
+        hist = ctx.iterate(n_iter)
+        gx = ctx.download_image()
+        it = ctx.iteration
+    ox, ohist = O.recon(y.astype(np.complex128), ocfg, n_iter, x0=x0)
+    return gx, ox, np.asarray(hist), np.asarray(ohist), it
+
+
+def check(gx, ox, gh, oh):
+    assert np.all(np.isfinite(gh))
+    assert rel_err(gx, ox) < TOL, rel_err(gx, ox)
+    np.testing.assert_allclose(gh, oh, rtol=TOL)
+
+
+def test_soft_threshold_hybrid_path(gpu):
+    d = dataset((24, 20, 16), 6)
+    gx, ox, gh, oh, it = run_both(d.y, (4, 4, 4), L.LLR_PROX_SOFT_THRESH, 5)
+    assert it == 5
+    check(gx, ox, gh, oh)
+    assert gh[-1] < gh[0]
+
+
+def test_hard_rank_c1_like(gpu):
+    """Config-1 shape class: 8^3 blocks, 17 volumes (Casorati 512 x 17), reduced volume."""
+    d = dataset((32, 32, 32), 17, accel=4.0, centre=8)
+    gx, ox, gh, oh, _ = run_both(d.y, (8, 8, 8), L.LLR_PROX_HARD_RANK, 4, rank=4)
+    check(gx, ox, gh, oh)
+
+
+def test_soft_c2_like(gpu):
+    """Config-2 shape class: 6^3 blocks, 61 volumes (Casorati 216 x 61), reduced volume."""
+    d = dataset((24, 24, 12), 61, accel=8.0, centre=6)
+    gx, ox, gh, oh, _ = run_both(d.y, (6, 6, 6), L.LLR_PROX_SOFT_THRESH, 4)
+    check(gx, ox, gh, oh)
+
+
+def test_element_wise_sampling_path(gpu):
+    """A sampling set that is not whole x-lines takes the element-wise (3-D FFT) path."""
+    d = dataset((16, 12, 8), 5)
+    rng = np.random.default_rng(3)
+    y = d.y.copy()
+    y[rng.random(y.shape) < 0.3] = 0
+    gx, ox, gh, oh, _ = run_both(y, (4, 4, 4), L.LLR_PROX_SOFT_THRESH, 4)
+    check(gx, ox, gh, oh)
+
+
+@pytest.mark.parametrize("element_wise", [False, True])
+def test_linear_corrections(gpu, element_wise):
+    d = dataset((16, 12, 10), 4)
+    rng = np.random.default_rng(4)
+    lk = rng.uniform(-2, 2, (4, 3)).astype(np.float32)
+    li = rng.uniform(-2, 2, (4, 3)).astype(np.float32)
+    y = d.y.copy()
+    if element_wise:
+        y[rng.random(y.shape) < 0.2] = 0
+    gx, ox, gh, oh, _ = run_both(y, (4, 4, 2), L.LLR_PROX_SOFT_THRESH, 3,
+                                 lin=(lk.astype(np.float64), li.astype(np.float64)))
+    check(gx, ox, gh, oh)
+
+
+def test_volume_not_divisible_by_block(gpu):
+    """Voxels outside floor(vol/block) blocks pass through the prox unchanged (block.rs:112-118)."""
+    d = dataset((20, 18, 14), 5)
+    gx, ox, gh, oh, _ = run_both(d.y, (8, 8, 8), L.LLR_PROX_SOFT_THRESH, 3)
+    check(gx, ox, gh, oh)
+
+
+def test_bounded_random_shift(gpu):
+    d = dataset((16, 16, 8), 5)
+    gx, ox, gh, oh, _ = run_both(d.y, (4, 4, 4), L.LLR_PROX_HARD_RANK, 3, rank=2, max_shift=(4, 4, 4))
+    check(gx, ox, gh, oh)
+
+
+def test_wavelet_term(gpu):
+    d = dataset((32, 24, 20), 4)
+    gx, ox, gh, oh, _ = run_both(d.y, (4, 4, 4), L.LLR_PROX_SOFT_THRESH, 3, wavelet=(0.002, 2, 2))
+    check(gx, ox, gh, oh)
+
+
+def test_subspace_llr(gpu):
+    vol, nq = (24, 16, 16), 13
+    d = make_dataset(vol, [(0, 1), (1000, 6), (2000, 6)], 3.0, 2, centre=6, mask_fn=O.vd_mask)
+    S = dti_subspace(d.b, d.g, 4, 2000, 1)
+    gx, ox, gh, oh, _ = run_both(d.y, (8, 8, 8), L.LLR_PROX_HARD_RANK, 3, rank=2, subspace=S)
+    check(gx, ox, gh, oh)
+
+
+def test_single_steps_and_sigma_max(gpu):
+    d = dataset((24, 20, 16), 6)
+    y = d.y
+    bs = (4, 4, 4)
+    ocfg = oracle_cfg(bs, "soft", seed=1)
+    x0 = O.zero_filled(y.astype(np.complex128), ocfg)
+    smax = O.sigma_max(x0, bs, (3, 5, 7))
+    p = ReconParams(vol_size=y.shape[:3], nq=y.shape[3], block_size=bs, prox_mode=L.LLR_PROX_SOFT_THRESH,
+                    lam=0.05 * smax, seed=1)
+    ocfg.lam = 0.05 * smax
+    with ReconContext(p) as ctx:
+        ctx.upload_kspace(y)
+        e, us = ctx.measurement_stats()
+        oe = O.calc_undersampling_factor(y)
+        assert abs(us - oe[0]) < 1e-9 * oe[0] and abs(e - oe[1]) < 1e-5 * oe[1]
+        ctx.init_zero_filled()
+        assert abs(ctx.sigma_max((3, 5, 7)) - smax) < 1e-4 * smax
+        ctx.prox((3, 5, 7))
+        px = O.llr_prox(x0, ocfg, (3, 5, 7))
+        assert rel_err(ctx.download_image(), px) < 5e-5
+        r = ctx.data_consistency()
+        k = O.signal_model(px, np.zeros((6, 3)), np.zeros((6, 3)), O.FORWARD)
+        k, err = O.hard_project(k, y.astype(np.complex128))
+        assert abs(r - err) < 1e-4 * err
+        xd = O.signal_model(k, np.zeros((6, 3)), np.zeros((6, 3)), O.INVERSE)
+        assert rel_err(ctx.download_image(), xd) < 5e-5
+
+
+def test_upload_download_round_trip_and_resume(gpu):
+    d = dataset((16, 16, 8), 5)
+    bs = (4, 4, 4)
+    p = ReconParams(vol_size=(16, 16, 8), nq=5, block_size=bs, prox_mode=L.LLR_PROX_HARD_RANK, rank=2, seed=9)
+    with ReconContext(p) as a:
+        a.upload_kspace(d.y)
+        a.init_zero_filled()
+        a.iterate(3)
+        mid = a.download_image()
+        a.iterate(2)
+        straight = a.download_image()
+        h_all = a.residual_history(5)
+    with ReconContext(p) as b:
+        b.upload_kspace(d.y)
+        b.upload_image(mid)
+        assert rel_err(b.download_image(), mid) < 1e-6
+        b.iteration = 3                     # checkpoint/resume: same shift sequence from it 3
+        b.iterate(2)
+        assert rel_err(b.download_image(), straight) < 1e-5
+        np.testing.assert_allclose(b.residual_history(2), h_all[3:], rtol=1e-5)
+
+
+def test_state_errors(gpu):
+    p = ReconParams(vol_size=(16, 16, 8), nq=3, block_size=(4, 4, 4), rank=1)
+    with ReconContext(p) as ctx:
+        with pytest.raises(llr_b200.LlrError) as e:
+            ctx.iterate(1)
+        assert e.value.status == L.LLR_ERR_STATE
+        with pytest.raises(llr_b200.LlrError):
+            ctx.download_image()
+
+
+def test_unsupported_casorati_is_reported(gpu):
+    p = ReconParams(vol_size=(64, 64, 64), nq=70, block_size=(8, 8, 8), rank=2)
+    with pytest.raises(llr_b200.LlrError) as e:
+        ReconContext(p)
+    assert e.value.status == L.LLR_ERR_UNSUPPORTED
