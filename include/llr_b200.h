@@ -121,6 +121,13 @@ int llr_download_image_dev(llr_ctx* ctx, llr_cf32* d_x);
 int llr_iterate(llr_ctx* ctx, int32_t n_iter, double* resid_hist);
 /* Enqueue n iterations on the context stream without synchronising (no history copy). */
 int llr_iterate_async(llr_ctx* ctx, int32_t n_iter);
+/* Same iterations, each stage captured as its own graph with CUDA events recorded on the
+ * context stream between stages.  stage_ms[5] (may be NULL) receives the summed device
+ * time of: LLR prox, wavelet, forward FFT, data consistency, inverse FFT; total_ms the
+ * device time from the first to the last event.  Synchronises. */
+int llr_iterate_profiled(llr_ctx* ctx, int32_t n_iter, double* stage_ms, double* total_ms);
+/* Device time of n single-graph iterations (events on the context stream). */
+int llr_iterate_timed(llr_ctx* ctx, int32_t n_iter, double* total_ms);
 int llr_get_iteration(const llr_ctx* ctx, int64_t* it);
 int llr_set_iteration(llr_ctx* ctx, int64_t it);
 /* Residual history of the last `count` iterations ending at the current one. */

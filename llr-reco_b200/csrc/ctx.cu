@@ -52,6 +52,11 @@ void drop_graph(llr_ctx* c) {
     cudaGraphDestroy(c->graph);
     c->have_graph = false;
   }
+  if (c->have_stages) {
+    for (int i = 0; i < 5; ++i)
+      if (c->stage_exec[i]) cudaGraphExecDestroy(c->stage_exec[i]);
+    c->have_stages = false;
+  }
 }
 
 int exec_fft(llr_ctx* c, float2* d, int dir, cudaStream_t s) {
@@ -535,6 +540,118 @@ static int build_graph(llr_ctx* c) {
   c->graph = graph;
   c->have_graph = true;
   return LLR_OK;
+}
+
+static int capture_stage(llr_ctx* c, int stage, cudaGraphExec_t* out) {
+  cudaStream_t s = c->stream;
+  *out = nullptr;
+  LLR_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  int st = LLR_OK;
+  switch (stage) {
+    case 0: st = prox_pass(c, s, nullptr, false, nullptr); break;
+    case 1: if (c->wavelet_on) st = wavelet_pass(c, s, 1.f); break;
+    case 2: st = exec_fft(c, c->d_x, CUFFT_FORWARD, s); break;
+    case 3:
+      st = dc_pass(c, s, 0);
+      if (st == LLR_OK)
+        st = launch_finalize(c->d_partials, n_partials(c), (double)c->load_scale, c->d_hist, c->hist_cap, c->d_iter,
+                             1, nullptr, s);
+      break;
+    case 4: st = exec_fft(c, c->d_x, CUFFT_INVERSE, s); break;
+  }
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamEndCapture(s, &graph);
+  if (st != LLR_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    return st;
+  }
+  if (e != cudaSuccess) return cuda_error(e, "cudaStreamEndCapture", __FILE__, __LINE__);
+  e = cudaGraphInstantiate(out, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return cuda_error(e, "cudaGraphInstantiate", __FILE__, __LINE__);
+  return LLR_OK;
+}
+
+int llr_iterate_profiled(llr_ctx* c, int32_t n, double* stage_ms, double* total_ms) {
+  if (!c) return set_error(LLR_ERR_INVALID, "null context");
+  if (n < 1) return set_error(LLR_ERR_INVALID, "need at least one iteration");
+  if (!c->have_kspace || !c->have_image) return set_error(LLR_ERR_STATE, "upload k-space and initialise the image");
+  if (c->cfg.subspace_rank > 0 && !c->d_S) return set_error(LLR_ERR_STATE, "subspace not uploaded");
+  LLR_CUDA_TRY(cudaSetDevice(c->device));
+  if (!c->have_stages) {
+    for (int i = 0; i < 5; ++i) {
+      int st = capture_stage(c, i, &c->stage_exec[i]);
+      if (st != LLR_OK) {
+        for (int j = 0; j < i; ++j) cudaGraphExecDestroy(c->stage_exec[j]);
+        return st;
+      }
+    }
+    c->have_stages = true;
+  }
+  std::vector<cudaEvent_t> ev((size_t)n * 6, nullptr);
+  int st = LLR_OK;
+  for (size_t i = 0; i < ev.size() && st == LLR_OK; ++i) {
+    cudaError_t e = cudaEventCreate(&ev[i]);
+    if (e != cudaSuccess) st = cuda_error(e, "cudaEventCreate", __FILE__, __LINE__);
+  }
+  for (int it = 0; it < n && st == LLR_OK; ++it) {
+    for (int k = 0; k < 5 && st == LLR_OK; ++k) {
+      cudaError_t e = cudaEventRecord(ev[(size_t)it * 6 + k], c->stream);
+      if (e == cudaSuccess) e = cudaGraphLaunch(c->stage_exec[k], c->stream);
+      if (e != cudaSuccess) st = cuda_error(e, "stage launch", __FILE__, __LINE__);
+    }
+    if (st == LLR_OK) {
+      cudaError_t e = cudaEventRecord(ev[(size_t)it * 6 + 5], c->stream);
+      if (e != cudaSuccess) st = cuda_error(e, "cudaEventRecord", __FILE__, __LINE__);
+    }
+  }
+  if (st == LLR_OK) {
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) st = cuda_error(e, "cudaStreamSynchronize", __FILE__, __LINE__);
+  }
+  if (st == LLR_OK) {
+    double acc[5] = {0, 0, 0, 0, 0};
+    for (int it = 0; it < n; ++it)
+      for (int k = 0; k < 5; ++k) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev[(size_t)it * 6 + k], ev[(size_t)it * 6 + k + 1]);
+        acc[k] += ms;
+      }
+    float tot = 0.f;
+    cudaEventElapsedTime(&tot, ev[0], ev[(size_t)(n - 1) * 6 + 5]);
+    if (stage_ms)
+      for (int k = 0; k < 5; ++k) stage_ms[k] = acc[k];
+    if (total_ms) *total_ms = tot;
+    c->h_iter += n;
+  }
+  for (auto e : ev)
+    if (e) cudaEventDestroy(e);
+  return st;
+}
+
+int llr_iterate_timed(llr_ctx* c, int32_t n, double* total_ms) {
+  if (!c) return set_error(LLR_ERR_INVALID, "null context");
+  LLR_CUDA_TRY(cudaSetDevice(c->device));
+  cudaEvent_t a, b;
+  LLR_CUDA_TRY(cudaEventCreate(&a));
+  LLR_CUDA_TRY(cudaEventCreate(&b));
+  int st = LLR_OK;
+  cudaError_t e = cudaEventRecord(a, c->stream);
+  if (e != cudaSuccess) st = cuda_error(e, "cudaEventRecord", __FILE__, __LINE__);
+  if (st == LLR_OK) st = llr_iterate_async(c, n);
+  if (st == LLR_OK) {
+    e = cudaEventRecord(b, c->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(b);
+    if (e != cudaSuccess) st = cuda_error(e, "cudaEventSynchronize", __FILE__, __LINE__);
+  }
+  if (st == LLR_OK) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    if (total_ms) *total_ms = ms;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return st;
 }
 
 int llr_iterate_async(llr_ctx* c, int32_t n) {

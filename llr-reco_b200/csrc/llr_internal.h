@@ -126,6 +126,8 @@ struct llr_ctx {
   cudaGraph_t graph;
   cudaGraphExec_t graph_exec;
   bool have_graph;
+  cudaGraphExec_t stage_exec[5];
+  bool have_stages;
   // measurement stats
   double total_energy;
   double undersampling;

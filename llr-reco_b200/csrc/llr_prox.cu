@@ -530,7 +530,11 @@ __global__ void __launch_bounds__(kLlrThreads) llr_subspace_kernel(BlockSource s
   float2* Ss = Z + (size_t)op.srank * L.ldc;                        // nq x srank
   constexpr int lda = NPMAX + 1;
   const int m = op.m, nq = op.nq, sr = op.srank;
-  for (int i = threadIdx.x; i < nq * sr; i += blockDim.x) Ss[i] = op.S[i];
+  // S is nq x srank column-major; keep it row-major (q, k) in shared memory.
+  for (int i = threadIdx.x; i < nq * sr; i += blockDim.x) {
+    const int q = i / sr, k = i - q * sr;
+    Ss[i] = op.S[q + (long long)nq * k];
+  }
   if (threadIdx.x == 0) block_shift(src, misc->shift);
   __syncthreads();
   int sh[3] = {misc->shift[0], misc->shift[1], misc->shift[2]};

@@ -100,6 +100,8 @@ SIGNATURES = {
     "llr_download_image_dev": (C.c_int, [P, P]),
     "llr_iterate": (C.c_int, [P, I32, PF64]),
     "llr_iterate_async": (C.c_int, [P, I32]),
+    "llr_iterate_profiled": (C.c_int, [P, I32, PF64, PF64]),
+    "llr_iterate_timed": (C.c_int, [P, I32, PF64]),
     "llr_get_iteration": (C.c_int, [P, C.POINTER(I64)]),
     "llr_set_iteration": (C.c_int, [P, I64]),
     "llr_get_residual_history": (C.c_int, [P, PF64, I32]),

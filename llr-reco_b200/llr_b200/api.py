@@ -40,7 +40,8 @@ class DeviceBuffer:
 
     @classmethod
     def from_array(cls, a: np.ndarray) -> "DeviceBuffer":
-        a = np.require(a, requirements=["A"])
+        """Copy ``a`` to the device in column-major order (the library's convention)."""
+        a = np.asfortranarray(a)
         b = cls(a.nbytes)
         check(lib.llr_memcpy_h2d(b.ptr, L.ptr(a), a.nbytes, None))
         check(lib.llr_stream_sync(None))
@@ -52,7 +53,9 @@ class DeviceBuffer:
         check(lib.llr_stream_sync(None))
 
     def download(self, a: np.ndarray) -> np.ndarray:
+        """Copy device bytes into ``a``, which must be column-major (or 1-D)."""
         assert a.nbytes <= self.nbytes
+        assert a.flags["F_CONTIGUOUS"], "download target must be column-major"
         check(lib.llr_stream_sync(None))
         check(lib.llr_memcpy_d2h(L.ptr(a), self.ptr, a.nbytes, None))
         check(lib.llr_stream_sync(None))
@@ -184,6 +187,19 @@ class ReconContext:
 
     def iterate_async(self, n: int) -> None:
         check(lib.llr_iterate_async(self.h, int(n)))
+
+    def iterate_timed(self, n: int) -> float:
+        """Device milliseconds of ``n`` single-graph iterations (CUDA events on the context stream)."""
+        ms = C.c_double()
+        check(lib.llr_iterate_timed(self.h, int(n), C.byref(ms)))
+        return ms.value
+
+    def iterate_profiled(self, n: int) -> tuple[np.ndarray, float]:
+        """Per-stage device milliseconds (prox, wavelet, FFT, DC, IFFT) summed over ``n`` iterations."""
+        st = np.zeros(5, dtype=np.float64)
+        tot = C.c_double()
+        check(lib.llr_iterate_profiled(self.h, int(n), st.ctypes.data_as(L.PF64), C.byref(tot)))
+        return st, tot.value
 
     @property
     def iteration(self) -> int:

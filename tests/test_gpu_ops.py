@@ -87,7 +87,7 @@ def test_soft_threshold_batch_matches_oracle(gpu, m, n):
     lam = float(np.median(s))
     d = DeviceBuffer.from_array(A)
     L.check(L.lib.llr_soft_threshold_batch_dev(m, n, lam, batch, d.ptr, None))
-    got = d.download(np.empty_like(A))
+    got = d.download(np.empty_like(A, order="F"))
     exp = O.low_rank_soft(A.astype(np.complex128), lam)
     assert rel_err(got, exp) < 5e-5
 
@@ -102,7 +102,7 @@ def test_zero_and_rank_deficient_blocks(gpu):
     assert rel_err(buf.reshape(m, n, batch, order="F"), A) < 1e-6
     d = DeviceBuffer.from_array(A)
     L.check(L.lib.llr_soft_threshold_batch_dev(m, n, 0.0, batch, d.ptr, None))
-    assert rel_err(d.download(np.empty_like(A)), A) < 1e-6
+    assert rel_err(d.download(np.empty_like(A, order="F")), A) < 1e-6
 
 
 def test_rhs_cdgmm_known_answer(gpu):
@@ -112,7 +112,7 @@ def test_rhs_cdgmm_known_answer(gpu):
     d = np.tile((np.arange(n) + 1.0)[:, None], (1, batch)).astype(np.float32)
     dA, dd = DeviceBuffer.from_array(A), DeviceBuffer.from_array(np.asfortranarray(d))
     assert L.lib.rhsCdgmmBatched(m, n, batch, dA.ptr, dd.ptr) == 0
-    got = dA.download(np.empty_like(A))
+    got = dA.download(np.empty_like(A, order="F"))
     exp = ((np.arange(n) + 1.0) * (1 + 1j))[None, :, None] * np.ones((m, 1, batch))
     np.testing.assert_array_equal(got, exp.astype(np.complex64))
 
@@ -199,7 +199,7 @@ def test_subspace_low_rank_matches_oracle(gpu, mode):
     dS, dX = DeviceBuffer.from_array(S), DeviceBuffer.from_array(X)
     L.check(L.lib.llr_subspace_low_rank_batch_dev(m, nq, srank, L.LLR_PROX_HARD_RANK if mode == "hard" else
                                                   L.LLR_PROX_SOFT_THRESH, rank, lam, dS.ptr, batch, dX.ptr, None))
-    got = dX.download(np.empty_like(X))
+    got = dX.download(np.empty_like(X, order="F"))
     exp = O.subspace_low_rank(X.astype(np.complex128), S.astype(np.complex128), mode, rank, lam)
     assert rel_err(got, exp) < 5e-5
 
@@ -250,7 +250,7 @@ def test_wavelet_denoise_matches_oracle(gpu, vol, moments, levels):
     alpha = 0.8
     d = DeviceBuffer.from_array(x)
     L.check(L.lib.llr_wavelet_denoise_dev(d.ptr, L.i32x3(vol), nvol, moments, levels, alpha, None))
-    got = d.download(np.empty_like(x))
+    got = d.download(np.empty_like(x, order="F"))
     bank = O.daubechies_bank(moments)
     exp = np.stack([O.wavelet_denoise(x[..., v].astype(np.complex128), alpha, bank, levels) for v in range(nvol)], -1)
     assert rel_err(got, exp) < 5e-5
@@ -267,7 +267,7 @@ def test_hard_project_matches_reference(gpu):
     import ctypes as C
     err = C.c_double()
     L.check(L.lib.llr_hard_project_dev(dx.ptr, dy.ptr, n, C.byref(err), None))
-    got = dx.download(np.empty_like(x))
+    got = dx.download(np.empty_like(x, order="F"))
     exp, e = O.hard_project(x, y)
     np.testing.assert_array_equal(got, exp)
     assert abs(err.value - e) <= 1e-6 * e
