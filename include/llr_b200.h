@@ -66,7 +66,8 @@ typedef struct llr_config {
   int32_t n_iter;             /* default iteration count (lib.rs:62)                 */
   uint64_t seed;              /* key of the counter-based shift RNG                  */
   int32_t device;             /* CUDA device ordinal                                 */
-  int32_t reserved[7];
+  int32_t eig_solver;         /* 0: tridiagonal + bisection (default); 1: Jacobi      */
+  int32_t reserved[6];
 } llr_config;
 
 /* ---- library / errors ------------------------------------------------------------ */

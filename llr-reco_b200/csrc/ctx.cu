@@ -180,6 +180,7 @@ static int prox_pass(llr_ctx* c, cudaStream_t s, const int* explicit_shift, bool
     ProxOp op;
     op.m = c->m; op.n = c->g.nq; op.mode = c->cfg.prox_mode; op.rank = c->cfg.rank; op.lambda = c->cfg.lambda;
     op.block_stat = block_stat;
+    op.eig_solver = c->cfg.eig_solver;
     LLR_TRY(launch_llr_prox(src, op, s));
   }
   if (block_stat || standalone) return LLR_OK;

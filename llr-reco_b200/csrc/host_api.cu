@@ -188,6 +188,7 @@ int llr_config_validate(const llr_config* c) {
   if (c->subspace_rank > 0 && c->prox_mode == LLR_PROX_HARD_RANK && c->rank > c->subspace_rank)
     return set_error(LLR_ERR_INVALID, "llr rank must be <= subspace rank (lib.rs:217)");
   if (!(c->wavelet_alpha >= 0.f)) return set_error(LLR_ERR_INVALID, "wavelet_alpha must be >= 0");
+  if (c->eig_solver != 0 && c->eig_solver != 1) return set_error(LLR_ERR_INVALID, "eig_solver must be 0 or 1");
   if (c->wavelet_alpha > 0.f && (c->wavelet_moments < 1 || c->wavelet_moments > 10))
     return set_error(LLR_ERR_INVALID, "wavelet_moments must be in [1, 10]");
   if (m < 1) return set_error(LLR_ERR_INVALID, "empty block");
@@ -339,6 +340,8 @@ int llr_un_lift_data_set_dev(llr_cf32* d_vol, int32_t nq, const llr_cf32* d_mat,
   return launch_lift((const float2*)d_vol, (float2*)d_mat, vs, nq, bs, sh, start, n, 1, (cudaStream_t)stream);
 }
 
+static int g_batch_eig_solver = 0;
+
 static int batch_prox(int m, int n, int mode, int rank, float lam, int batch, llr_cf32* d, void* stream) {
   if (!d || m < 1 || n < 1 || batch < 0) return set_error(LLR_ERR_INVALID, "bad matrix batch arguments");
   BlockSource src;
@@ -348,6 +351,7 @@ static int batch_prox(int m, int n, int mode, int rank, float lam, int batch, ll
   src.nblocks = batch;
   ProxOp op;
   op.m = m; op.n = n; op.mode = mode; op.rank = rank; op.lambda = lam; op.block_stat = nullptr;
+  op.eig_solver = g_batch_eig_solver;
   return launch_llr_prox(src, op, (cudaStream_t)stream);
 }
 

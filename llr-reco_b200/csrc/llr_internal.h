@@ -36,6 +36,7 @@ struct ProxOp {
   int rank;
   float lambda;
   float* block_stat;   // when non-null: write the largest Gram eigenvalue, skip the update
+  int eig_solver;      // 0: tridiagonal + bisection + inverse iteration; 1: Jacobi
 };
 
 int launch_llr_prox(const BlockSource& src, const ProxOp& op, cudaStream_t stream);

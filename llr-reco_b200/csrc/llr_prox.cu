@@ -23,7 +23,22 @@ struct SmemLayout {
   int ldc;        // leading dimension of C in shared memory (odd)
   int np;         // padded n for Gram tiles
   int ksplit;     // Gram K-split factor
-  size_t off_rot, off_pair, off_ev, off_g, off_act, off_A, off_V, off_scr, off_C, total;
+  size_t off_rot, off_pair, off_ev, off_g, off_act, off_A, off_V, off_scr, off_C, off_trd, total;
+};
+
+// Tridiagonal-path scratch (NPMAX-sized vectors and the real eigenvectors of T').
+template <int NPMAX>
+struct TrdSmem {
+  float2 u[NPMAX];      // current Householder vector
+  float2 p[NPMAX];      // tau * A22 u
+  float2 e[NPMAX];      // complex sub-diagonal of T
+  float2 delta[NPMAX];  // unitary diagonal making T' = D^H T D real
+  float d[NPMAX];       // diagonal of T
+  float ae[NPMAX];      // |e|
+  float e2[NPMAX];      // |e|^2
+  float tau[NPMAX];     // reflector scalars
+  float lam[NPMAX];     // active eigenvalues (ascending), perturbed for inverse iteration
+  float Y[NPMAX * NPMAX];  // eigenvectors of T', column a at Y[a * NPMAX]
 };
 
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
@@ -47,6 +62,7 @@ SmemLayout make_layout(int m, int n) {
   L.off_scr = off;
   if (L.ksplit > 1) off = align16(off + sizeof(float2) * (size_t)L.ksplit * L.np * L.np);
   L.off_C = off; off = align16(off + sizeof(float2) * (size_t)n * L.ldc);
+  L.off_trd = off; off = align16(off + sizeof(TrdSmem<NPMAX>));
   L.total = off;
   return L;
 }
@@ -56,7 +72,12 @@ struct Misc {
   float normF;
   int n_active;
   int shift[3];
-  int pad;
+  int n_below;      // eigenvalues below the threshold (tridiagonal path)
+  int ra;           // active eigenpairs (tridiagonal path)
+  int fail;         // tridiagonal path rejected -> Jacobi fallback
+  float tnorm;      // max |Gershgorin bound| of T'
+  float gl, gu;     // Gershgorin interval
+  float pivmin;
   float red[32];
 };
 
@@ -417,6 +438,358 @@ __device__ void apply_W(float2* Cs, int ldc, int m, int n, const float2* W) {
   __syncthreads();
 }
 
+// =======================================================================================
+// Tridiagonal eigen path.  Householder reduction of the Hermitian Gram matrix to
+// tridiagonal T (H = I - tau u u^H, tau real), a unitary diagonal D making T' = D^H T D
+// real, Sturm-count multisection for only the eigenvalues that the singular-value map keeps
+// (above lambda^2, or the top `rank`), inverse iteration for their eigenvectors, modified
+// Gram-Schmidt plus a residual check, and back-transformation V = Q D Y.  About n^3 complex
+// flops in total against sweeps * 8 n^3 for Jacobi; blocks whose eigenvectors fail the
+// residual check take the Jacobi path.
+// =======================================================================================
+template <int NPMAX>
+__device__ void hermitian_tridiag(float2* A, int n, TrdSmem<NPMAX>* T, float* red) {
+  constexpr int lda = NPMAX + 1;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nwarps = blockDim.x >> 5;
+  for (int k = 0; k + 2 < n; ++k) {
+    const int L = n - k - 1;
+    if (warp == 0) {
+      const int i0 = lane, i1 = lane + 32;
+      float2 x0 = make_float2(0.f, 0.f), x1 = make_float2(0.f, 0.f);
+      if (i0 < L) x0 = A[(k + 1 + i0) * lda + k];
+      if (i1 < L) x1 = A[(k + 1 + i1) * lda + k];
+      float s2 = cabs2(x0) + cabs2(x1);
+      for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+      const float ax = __shfl_sync(0xffffffffu, x0.x, 0), ay = __shfl_sync(0xffffffffu, x0.y, 0);
+      const float xn = sqrtf(s2);
+      const float aa = sqrtf(ax * ax + ay * ay);
+      const float phx = aa > 0.f ? ax / aa : 1.f, phy = aa > 0.f ? ay / aa : 0.f;
+      const float2 u0 = make_float2(ax + phx * xn, ay + phy * xn);
+      const float un2 = s2 - aa * aa + cabs2(u0);
+      const float t = (xn > 0.f && un2 > 0.f) ? 2.f / un2 : 0.f;
+      if (lane == 0) {
+        T->tau[k] = t;
+        T->e[k] = make_float2(-phx * xn, -phy * xn);
+        A[(k + 1) * lda + k] = u0;  // column k now stores u_k for the back-transformation
+      }
+      if (i0 < L) T->u[i0] = (i0 == 0) ? u0 : x0;
+      if (i1 < L) T->u[i1] = x1;
+    }
+    __syncthreads();
+    const float t = T->tau[k];
+    if (t != 0.f) {
+      // p = t * A22 u : four threads per row
+      const int row = tid >> 2, part = tid & 3;
+      float2 acc = make_float2(0.f, 0.f);
+      if (row < L) {
+        const float2* Ar = A + (k + 1 + row) * lda + (k + 1);
+        for (int j = part; j < L; j += 4) cfma(acc, Ar[j], T->u[j]);
+      }
+      acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 1);
+      acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 1);
+      acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 2);
+      acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 2);
+      float dp = 0.f;
+      if (row < L && part == 0) {
+        const float2 pv = cscale(acc, t);
+        T->p[row] = pv;
+        const float2 uv = T->u[row];
+        dp = uv.x * pv.x + uv.y * pv.y;  // Re(conj(u) p)
+      }
+      for (int o = 16; o > 0; o >>= 1) dp += __shfl_xor_sync(0xffffffffu, dp, o);
+      if (lane == 0) red[warp] = dp;
+      __syncthreads();
+      float up = 0.f;
+      for (int w = 0; w < nwarps; ++w) up += red[w];
+      const float K = 0.5f * t * up;
+      // A22 -= u w^H + w u^H,  w = p - K u
+      const int tj = tid & 15, ti = tid >> 4;
+      for (int i = ti; i < L; i += 16) {
+        const float2 ui = T->u[i];
+        const float2 wi = csub(T->p[i], cscale(ui, K));
+        float2* Ar = A + (k + 1 + i) * lda + (k + 1);
+        for (int j = tj; j < L; j += 16) {
+          const float2 uj = T->u[j];
+          const float2 wj = csub(T->p[j], cscale(uj, K));
+          Ar[j] = csub(csub(Ar[j], cmul_bc(ui, wj)), cmul_bc(wi, uj));
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (tid < n) T->d[tid] = A[tid * lda + tid].x;
+  if (tid == 0) {
+    if (n >= 2) T->e[n - 2] = A[(n - 1) * lda + n - 2];
+    for (int k = n - 2; k < n; ++k)
+      if (k >= 0) T->tau[k] = 0.f;
+  }
+  __syncthreads();
+}
+
+// Sturm count: number of eigenvalues of the real tridiagonal (d, e2 = offdiag^2) below x.
+__device__ __forceinline__ int sturm_count(const float* d, const float* e2, int n, float x, float pivmin) {
+  float q = d[0] - x;
+  if (fabsf(q) <= pivmin) q = -pivmin;
+  int c = q < 0.f;
+  for (int i = 1; i < n; ++i) {
+    q = d[i] - x - e2[i - 1] / q;
+    if (fabsf(q) <= pivmin) q = -pivmin;
+    c += q < 0.f;
+  }
+  return c;
+}
+
+// Real form T' (D), Gershgorin interval, and the active index range (eigenvalues
+// n_below .. n_below + ra - 1 in ascending order).
+template <int NPMAX>
+__device__ void tridiag_setup(TrdSmem<NPMAX>* T, int n, int mode, int rank, float lam, Misc* misc) {
+  if (threadIdx.x == 0) {
+    float2 dl = make_float2(1.f, 0.f);
+    float e2max = 0.f;
+    for (int k = 0; k < n; ++k) {
+      T->delta[k] = dl;
+      if (k + 1 < n) {
+        const float2 ek = T->e[k];
+        const float a = sqrtf(cabs2(ek));
+        T->ae[k] = a;
+        T->e2[k] = a * a;
+        e2max = fmaxf(e2max, a * a);
+        if (a > 0.f) dl = cmul(dl, make_float2(ek.x / a, ek.y / a));
+      } else {
+        T->ae[k] = 0.f;
+        T->e2[k] = 0.f;
+      }
+    }
+    float gl = 3.0e38f, gu = -3.0e38f;
+    for (int k = 0; k < n; ++k) {
+      const float r = (k > 0 ? T->ae[k - 1] : 0.f) + (k + 1 < n ? T->ae[k] : 0.f);
+      gl = fminf(gl, T->d[k] - r);
+      gu = fmaxf(gu, T->d[k] + r);
+    }
+    const float tn = fmaxf(fabsf(gl), fabsf(gu));
+    gl -= 4.f * 1.1920929e-7f * tn * n + 1e-30f;
+    gu += 4.f * 1.1920929e-7f * tn * n + 1e-30f;
+    misc->gl = gl;
+    misc->gu = gu;
+    misc->tnorm = tn;
+    misc->pivmin = 1.1754944e-38f * fmaxf(1.f, e2max);
+    int nb;
+    if (mode == LLR_PROX_HARD_RANK) nb = max(0, n - rank);
+    else if (!(lam > 0.f)) nb = 0;
+    else nb = sturm_count(T->d, T->e2, n, lam * lam, misc->pivmin);
+    misc->n_below = nb;
+    misc->ra = n - nb;
+    misc->fail = 0;
+  }
+  __syncthreads();
+}
+
+// Multisection: groups of 8 lanes refine eigenvalue j by 9-way splits (warp-uniform loop).
+template <int NPMAX>
+__device__ void tridiag_eigenvalues(TrdSmem<NPMAX>* T, int n, int j0, int count, const Misc* misc) {
+  const int lane = threadIdx.x & 31;
+  const int gl8 = lane & 7;
+  const int group = threadIdx.x >> 3;
+  const int ngroups = blockDim.x >> 3;
+  for (int base = 0; base < count; base += ngroups) {
+    const int a = base + group;
+    const bool act = a < count;
+    const int j = j0 + (act ? a : 0);
+    float lo = misc->gl, hi = misc->gu;
+    for (int round = 0; round < 14; ++round) {
+      const bool conv = !act || (hi - lo) <= 2.4e-7f * fmaxf(fabsf(lo), fabsf(hi)) + misc->pivmin;
+      if (__all_sync(0xffffffffu, conv)) break;
+      const float x = lo + (hi - lo) * (float)(gl8 + 1) * (1.f / 9.f);
+      const bool le = act ? (sturm_count(T->d, T->e2, n, x, misc->pivmin) <= j) : true;
+      const unsigned bal = __ballot_sync(0xffffffffu, le);
+      const int nt = __popc((bal >> (lane & 24)) & 0xffu);
+      const float nlo = nt > 0 ? lo + (hi - lo) * (float)nt * (1.f / 9.f) : lo;
+      const float nhi = nt < 8 ? lo + (hi - lo) * (float)(nt + 1) * (1.f / 9.f) : hi;
+      lo = nlo;
+      hi = nhi;
+    }
+    if (act && gl8 == 0) T->lam[a] = 0.5f * (lo + hi);
+  }
+  __syncthreads();
+}
+
+// Inverse iteration (one thread per active eigenvalue) on T' - lambda I with partial
+// pivoting; three solves from a deterministic start vector.
+template <int NPMAX>
+__device__ void tridiag_vectors(TrdSmem<NPMAX>* T, int n, int ra, Misc* misc) {
+  const float eps = 1.1920929e-7f;
+  const float tiny = eps * fmaxf(misc->tnorm, 1e-30f);
+  if (threadIdx.x == 0) {  // separate (near-)equal eigenvalues (LAPACK stein convention)
+    const float sep = 10.f * eps * fmaxf(misc->tnorm, 1e-30f);
+    for (int a = 1; a < ra; ++a)
+      if (T->lam[a] - T->lam[a - 1] < sep) T->lam[a] = T->lam[a - 1] + sep;
+  }
+  __syncthreads();
+  for (int a = threadIdx.x; a < ra; a += blockDim.x) {
+    const float lam = T->lam[a];
+    float dd[NPMAX], du[NPMAX], du2[NPMAX], dl[NPMAX], b[NPMAX];
+    unsigned long long piv = 0ull;
+    for (int i = 0; i < n; ++i) {
+      dd[i] = T->d[i] - lam;
+      du[i] = (i + 1 < n) ? T->ae[i] : 0.f;
+      dl[i] = du[i];
+      du2[i] = 0.f;
+    }
+    for (int i = 0; i + 1 < n; ++i) {
+      if (fabsf(dd[i]) >= fabsf(dl[i])) {
+        if (fabsf(dd[i]) < tiny) dd[i] = copysignf(tiny, dd[i] == 0.f ? 1.f : dd[i]);
+        const float f = dl[i] / dd[i];
+        dl[i] = f;
+        dd[i + 1] -= f * du[i];
+      } else {
+        const float f = dd[i] / dl[i];
+        dd[i] = dl[i];
+        dl[i] = f;
+        const float tmp = du[i];
+        du[i] = dd[i + 1];
+        dd[i + 1] = tmp - f * dd[i + 1];
+        if (i + 2 < n) {
+          du2[i] = du[i + 1];
+          du[i + 1] = -f * du[i + 1];
+        }
+        piv |= (1ull << i);
+      }
+    }
+    if (fabsf(dd[n - 1]) < tiny) dd[n - 1] = copysignf(tiny, dd[n - 1] == 0.f ? 1.f : dd[n - 1]);
+    uint64_t h = llr_splitmix64(0x1234567ull + (uint64_t)a);
+    for (int i = 0; i < n; ++i) {
+      h = llr_splitmix64(h);
+      b[i] = (float)((h >> 40) & 0xffffff) * (1.f / 16777216.f) - 0.5f;
+    }
+    for (int it = 0; it < 3; ++it) {
+      for (int i = 0; i + 1 < n; ++i) {
+        if (piv & (1ull << i)) {
+          const float t = b[i];
+          b[i] = b[i + 1];
+          b[i + 1] = t - dl[i] * b[i];
+        } else {
+          b[i + 1] -= dl[i] * b[i];
+        }
+      }
+      b[n - 1] /= dd[n - 1];
+      if (n >= 2) b[n - 2] = (b[n - 2] - du[n - 2] * b[n - 1]) / dd[n - 2];
+      for (int i = n - 3; i >= 0; --i) b[i] = (b[i] - du[i] * b[i + 1] - du2[i] * b[i + 2]) / dd[i];
+      float mx = 0.f;
+      for (int i = 0; i < n; ++i) mx = fmaxf(mx, fabsf(b[i]));
+      const float sc = mx > 0.f ? 1.f / mx : 1.f;
+      for (int i = 0; i < n; ++i) b[i] *= sc;
+    }
+    for (int i = 0; i < n; ++i) T->Y[a * NPMAX + i] = b[i];
+  }
+  __syncthreads();
+  // modified Gram-Schmidt over the active vectors + residual check (warp 0)
+  if ((threadIdx.x >> 5) == 0) {
+    const int lane = threadIdx.x & 31;
+    const float tol = 2e-5f * fmaxf(misc->tnorm, 1e-30f);
+    int bad = 0;
+    for (int a = 0; a < ra; ++a) {
+      float* y = T->Y + a * NPMAX;
+      float y0 = lane < n ? y[lane] : 0.f, y1 = lane + 32 < n ? y[lane + 32] : 0.f;
+      for (int c = 0; c < a; ++c) {
+        const float* z = T->Y + c * NPMAX;
+        const float z0 = lane < n ? z[lane] : 0.f, z1 = lane + 32 < n ? z[lane + 32] : 0.f;
+        float dp = y0 * z0 + y1 * z1;
+        for (int o = 16; o > 0; o >>= 1) dp += __shfl_xor_sync(0xffffffffu, dp, o);
+        y0 -= dp * z0;
+        y1 -= dp * z1;
+      }
+      float nn = y0 * y0 + y1 * y1;
+      for (int o = 16; o > 0; o >>= 1) nn += __shfl_xor_sync(0xffffffffu, nn, o);
+      const float inv = nn > 0.f ? rsqrtf(nn) : 0.f;
+      y0 *= inv;
+      y1 *= inv;
+      if (lane < n) y[lane] = y0;
+      if (lane + 32 < n) y[lane + 32] = y1;
+      __syncwarp();
+      // residual |T' y - lambda y|
+      const float lam = T->lam[a];
+      float r2 = 0.f;
+      for (int h = 0; h < 2; ++h) {
+        const int i = lane + 32 * h;
+        if (i < n) {
+          float r = (T->d[i] - lam) * y[i];
+          if (i > 0) r += T->ae[i - 1] * y[i - 1];
+          if (i + 1 < n) r += T->ae[i] * y[i + 1];
+          r2 += r * r;
+        }
+      }
+      for (int o = 16; o > 0; o >>= 1) r2 += __shfl_xor_sync(0xffffffffu, r2, o);
+      if (!(nn > 0.f) || !(sqrtf(r2) <= tol)) bad = 1;
+      __syncwarp();
+    }
+    if (lane == 0) misc->fail = bad;
+  }
+  __syncthreads();
+}
+
+// V[:, a] = Q D y_a (complex), one warp per vector.
+template <int NPMAX>
+__device__ void tridiag_backtransform(const float2* A, TrdSmem<NPMAX>* T, float2* V, int n, int ra) {
+  constexpr int lda = NPMAX + 1;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int a = warp; a < ra; a += nw) {
+    const float* y = T->Y + a * NPMAX;
+    float2 v0 = make_float2(0.f, 0.f), v1 = make_float2(0.f, 0.f);
+    const int i0 = lane, i1 = lane + 32;
+    if (i0 < n) v0 = cscale(T->delta[i0], y[i0]);
+    if (i1 < n) v1 = cscale(T->delta[i1], y[i1]);
+    for (int k = n - 3; k >= 0; --k) {
+      const float t = T->tau[k];
+      if (t == 0.f) continue;
+      // u_k lives in column k of A below the diagonal (rows k+1 .. n-1), with u_k[0] at row k+1
+      // replaced by the value kept in column k during the reduction.
+      const float2 u0 = (i0 > k && i0 < n) ? A[i0 * lda + k] : make_float2(0.f, 0.f);
+      const float2 u1 = (i1 > k && i1 < n) ? A[i1 * lda + k] : make_float2(0.f, 0.f);
+      float2 s = cadd(cmulc(u0, v0), cmulc(u1, v1));
+      for (int o = 16; o > 0; o >>= 1) {
+        s.x += __shfl_xor_sync(0xffffffffu, s.x, o);
+        s.y += __shfl_xor_sync(0xffffffffu, s.y, o);
+      }
+      s = cscale(s, t);
+      v0 = csub(v0, cmul(u0, s));
+      v1 = csub(v1, cmul(u1, s));
+    }
+    if (i0 < n) V[i0 * lda + a] = v0;
+    if (i1 < n) V[i1 * lda + a] = v1;
+  }
+  __syncthreads();
+}
+
+// C <- (C V_a) diag(g) V_a^H for ra <= RM active vectors: one thread owns whole rows, so
+// rows are rewritten in place without a barrier.
+template <int NPMAX, int RM>
+__device__ void apply_lowrank_rows(float2* Cs, int ldc, int m, int n, const float2* V, const float* g, int ra) {
+  constexpr int lda = NPMAX + 1;
+  for (int r = threadIdx.x; r < m; r += blockDim.x) {
+    float2 t[RM];
+#pragma unroll
+    for (int a = 0; a < RM; ++a) t[a] = make_float2(0.f, 0.f);
+    for (int k = 0; k < n; ++k) {
+      const float2 c = Cs[k * ldc + r];
+#pragma unroll
+      for (int a = 0; a < RM; ++a)
+        if (a < ra) cfma(t[a], c, V[k * lda + a]);
+    }
+#pragma unroll
+    for (int a = 0; a < RM; ++a)
+      if (a < ra) t[a] = cscale(t[a], g[a]);
+    for (int q = 0; q < n; ++q) {
+      float2 c = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int a = 0; a < RM; ++a)
+        if (a < ra) cfma_cb(c, t[a], V[q * lda + a]);
+      Cs[q * ldc + r] = c;
+    }
+  }
+  __syncthreads();
+}
+
 template <int NPMAX, int TG>
 __global__ void __launch_bounds__(kLlrThreads) llr_prox_kernel(BlockSource src, ProxOp op, SmemLayout L) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -430,6 +803,7 @@ __global__ void __launch_bounds__(kLlrThreads) llr_prox_kernel(BlockSource src, 
   float2* V = reinterpret_cast<float2*>(smem + L.off_V);
   float2* scr = reinterpret_cast<float2*>(smem + L.off_scr);
   float2* Cs = reinterpret_cast<float2*>(smem + L.off_C);
+  TrdSmem<NPMAX>* trd = reinterpret_cast<TrdSmem<NPMAX>*>(smem + L.off_trd);
   constexpr int lda = NPMAX + 1;
   const int m = op.m, n = op.n;
 
@@ -441,23 +815,67 @@ __global__ void __launch_bounds__(kLlrThreads) llr_prox_kernel(BlockSource src, 
     gather_block(src, blk, sh, m, n, Cs, L.ldc);
     __syncthreads();
     gram<NPMAX, TG>(Cs, L.ldc, m, n, A, scr, L.ksplit);
-    jacobi<NPMAX>(A, V, n, rot, pairs, misc, 16);
-    if (op.block_stat) {
-      if (threadIdx.x == 0) {
-        float mx = 0.f;
-        for (int i = 0; i < n; ++i) mx = fmaxf(mx, A[i * lda + i].x);
-        op.block_stat[blk] = mx;
+    bool use_jacobi = op.eig_solver == 1;
+    if (!use_jacobi) {
+      hermitian_tridiag<NPMAX>(A, n, trd, misc->red);
+      if (op.block_stat) {
+        tridiag_setup<NPMAX>(trd, n, LLR_PROX_HARD_RANK, 1, 0.f, misc);
+        tridiag_eigenvalues<NPMAX>(trd, n, n - 1, 1, misc);
+        if (threadIdx.x == 0) op.block_stat[blk] = trd->lam[0];
+        __syncthreads();
+        continue;
       }
-      __syncthreads();
-      continue;
+      tridiag_setup<NPMAX>(trd, n, op.mode, op.rank, op.lambda, misc);
+      const int ra = misc->ra, nb = misc->n_below;
+      if (ra == n && op.mode == LLR_PROX_HARD_RANK) {
+        // rank >= n: identity
+      } else if (ra == 0) {
+        for (int i = threadIdx.x; i < n * L.ldc; i += blockDim.x) Cs[i] = make_float2(0.f, 0.f);
+        __syncthreads();
+      } else {
+        tridiag_eigenvalues<NPMAX>(trd, n, nb, ra, misc);
+        tridiag_vectors<NPMAX>(trd, n, ra, misc);
+        if (misc->fail) {
+          use_jacobi = true;
+          gram<NPMAX, TG>(Cs, L.ldc, m, n, A, scr, L.ksplit);
+        } else {
+          tridiag_backtransform<NPMAX>(A, trd, V, n, ra);
+          if (threadIdx.x < ra) {
+            float gv = 1.f;
+            if (op.mode != LLR_PROX_HARD_RANK) {
+              const float sv = sqrtf(fmaxf(trd->lam[threadIdx.x], 0.f));
+              gv = (sv > op.lambda) ? (1.f - op.lambda / sv) : 0.f;
+            }
+            g[threadIdx.x] = gv;
+            act[threadIdx.x] = threadIdx.x;
+          }
+          __syncthreads();
+          if (ra <= 8) {
+            apply_lowrank_rows<NPMAX, 8>(Cs, L.ldc, m, n, V, g, ra);
+          } else {
+            form_W(A, V, lda, n, g, act, ra);
+            apply_W<NPMAX, TG>(Cs, L.ldc, m, n, A);
+          }
+        }
+      }
     }
-    singular_map(A, lda, n, op.mode, op.rank, op.lambda, ev, g, act, misc);
-    const int na = misc->n_active;
-    if (na == n && op.mode == LLR_PROX_HARD_RANK) {
-      // rank >= n: the projector is the identity; data pass through unchanged.
-    } else {
-      form_W(A, V, lda, n, g, act, na);
-      apply_W<NPMAX, TG>(Cs, L.ldc, m, n, A);
+    if (use_jacobi) {
+      jacobi<NPMAX>(A, V, n, rot, pairs, misc, 16);
+      if (op.block_stat) {
+        if (threadIdx.x == 0) {
+          float mx = 0.f;
+          for (int i = 0; i < n; ++i) mx = fmaxf(mx, A[i * lda + i].x);
+          op.block_stat[blk] = mx;
+        }
+        __syncthreads();
+        continue;
+      }
+      singular_map(A, lda, n, op.mode, op.rank, op.lambda, ev, g, act, misc);
+      const int na = misc->n_active;
+      if (!(na == n && op.mode == LLR_PROX_HARD_RANK)) {
+        form_W(A, V, lda, n, g, act, na);
+        apply_W<NPMAX, TG>(Cs, L.ldc, m, n, A);
+      }
     }
     scatter_block(src, blk, sh, m, n, Cs, L.ldc);
     __syncthreads();

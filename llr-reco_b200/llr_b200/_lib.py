@@ -53,7 +53,8 @@ class llr_config(C.Structure):
         ("n_iter", C.c_int32),
         ("seed", C.c_uint64),
         ("device", C.c_int32),
-        ("reserved", C.c_int32 * 7),
+        ("eig_solver", C.c_int32),
+        ("reserved", C.c_int32 * 6),
     ]
 
 

@@ -114,6 +114,7 @@ class ReconParams:
     n_iter: int = 60
     seed: int = 0
     device: int = 0
+    eig_solver: int = 0
 
     def to_c(self) -> L.llr_config:
         c = L.llr_config()
@@ -132,6 +133,7 @@ class ReconParams:
         c.n_iter = int(self.n_iter)
         c.seed = int(self.seed)
         c.device = int(self.device)
+        c.eig_solver = int(self.eig_solver)
         return c
 
 

@@ -30,7 +30,7 @@ def oracle_cfg(bs, mode, rank=0, lam=0.0, seed=0, **kw):
 
 
 def run_both(y, bs, mode, n_iter, rank=2, lam_rel=0.02, seed=5, lin=None, wavelet=None, subspace=None,
-             max_shift=None):
+             max_shift=None, eig_solver=0):
     nx, ny, nz, nq = y.shape
     ocfg = oracle_cfg(bs, "hard" if mode == L.LLR_PROX_HARD_RANK else "soft", rank=rank, seed=seed,
                       max_rand_shift=max_shift)
@@ -46,7 +46,7 @@ def run_both(y, bs, mode, n_iter, rank=2, lam_rel=0.02, seed=5, lin=None, wavele
     if wavelet is not None:
         ocfg.wavelet_alpha, ocfg.wavelet_moments, ocfg.wavelet_levels = wavelet
     p = ReconParams(vol_size=(nx, ny, nz), nq=nq, block_size=bs, prox_mode=mode, rank=rank, lam=lam, seed=seed,
-                    max_rand_shift=max_shift,
+                    max_rand_shift=max_shift, eig_solver=eig_solver,
                     subspace_rank=0 if subspace is None else subspace.shape[1])
     if wavelet is not None:
         p.wavelet_alpha, p.wavelet_moments, p.wavelet_levels = wavelet
@@ -80,17 +80,20 @@ def test_soft_threshold_hybrid_path(gpu):
     assert gh[-1] < gh[0]
 
 
-def test_hard_rank_c1_like(gpu):
+@pytest.mark.parametrize("eig_solver", [0, 1])
+def test_hard_rank_c1_like(gpu, eig_solver):
     """Config-1 shape class: 8^3 blocks, 17 volumes (Casorati 512 x 17), reduced volume."""
     d = dataset((32, 32, 32), 17, accel=4.0, centre=8)
-    gx, ox, gh, oh, _ = run_both(d.y, (8, 8, 8), L.LLR_PROX_HARD_RANK, 4, rank=4)
+    gx, ox, gh, oh, _ = run_both(d.y, (8, 8, 8), L.LLR_PROX_HARD_RANK, 4, rank=4, eig_solver=eig_solver)
     check(gx, ox, gh, oh)
 
 
-def test_soft_c2_like(gpu):
-    """Config-2 shape class: 6^3 blocks, 61 volumes (Casorati 216 x 61), reduced volume."""
+@pytest.mark.parametrize("eig_solver", [0, 1])
+def test_soft_c2_like(gpu, eig_solver):
+    """Config-2 shape class: 6^3 blocks, 61 volumes (Casorati 216 x 61), reduced volume; both
+    eigen-solvers (tridiagonal + bisection, Jacobi)."""
     d = dataset((24, 24, 12), 61, accel=8.0, centre=6)
-    gx, ox, gh, oh, _ = run_both(d.y, (6, 6, 6), L.LLR_PROX_SOFT_THRESH, 4)
+    gx, ox, gh, oh, _ = run_both(d.y, (6, 6, 6), L.LLR_PROX_SOFT_THRESH, 4, eig_solver=eig_solver)
     check(gx, ox, gh, oh)
 
 
