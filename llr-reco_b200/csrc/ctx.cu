@@ -73,6 +73,10 @@ int upload_tables(llr_ctx* c) {
   std::vector<float2> h(2 * nt);
   phase_tables_host(dims, c->g.nq, c->lin_ksp.data(), h.data());
   phase_tables_host(dims, c->g.nq, c->lin_img.data(), h.data() + nt);
+  c->ph_uniform = 1;
+  for (int q = 1; q < c->g.nq; ++q)
+    for (int a = 0; a < 3; ++a)
+      if (c->lin_ksp[3 * q + a] != c->lin_ksp[a]) c->ph_uniform = 0;
   LLR_CUDA_TRY(cudaMemcpyAsync(c->d_ph_ksp, h.data(), sizeof(float2) * nt, cudaMemcpyHostToDevice, c->stream));
   LLR_CUDA_TRY(cudaMemcpyAsync(c->d_ph_img, h.data() + nt, sizeof(float2) * nt, cudaMemcpyHostToDevice, c->stream));
   LLR_CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -156,6 +160,9 @@ static BlockSource make_source(llr_ctx* c, const int* explicit_shift, float stor
   s.ph = ctx_phase(c, c->d_ph_ksp, !c->hybrid);
   s.store_phase = 1;
   s.store_scale = 1.f;
+  s.ph_uniform = c->ph_uniform;
+  s.blk_list = nullptr;
+  s.blk_count = nullptr;
   return s;
 }
 
@@ -181,6 +188,8 @@ static int prox_pass(llr_ctx* c, cudaStream_t s, const int* explicit_shift, bool
     op.m = c->m; op.n = c->g.nq; op.mode = c->cfg.prox_mode; op.rank = c->cfg.rank; op.lambda = c->cfg.lambda;
     op.block_stat = block_stat;
     op.eig_solver = c->cfg.eig_solver;
+    op.fb_list = c->d_fb;
+    op.fb_count = c->d_fb + std::max<long long>(1, c->nblocks);
     LLR_TRY(launch_llr_prox(src, op, s));
   }
   if (block_stat || standalone) return LLR_OK;
@@ -277,6 +286,7 @@ int llr_ctx_create(const llr_config* cfg, llr_ctx** out) {
   if ((st = dalloc(&c->d_hist, (size_t)c->hist_cap))) return fail(st);
   if ((st = dalloc(&c->d_iter, 1))) return fail(st);
   if ((st = dalloc(&c->d_block_stat, (size_t)std::max<long long>(1, c->nblocks)))) return fail(st);
+  if ((st = dalloc(&c->d_fb, (size_t)std::max<long long>(1, c->nblocks) + 1))) return fail(st);
   e = cudaMemsetAsync(c->d_iter, 0, sizeof(long long), c->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(c->d_hist, 0, sizeof(double) * c->hist_cap, c->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(c->d_x, 0, sizeof(float2) * E, c->stream);
@@ -310,7 +320,7 @@ int llr_ctx_destroy(llr_ctx* c) {
   if (c->have_plan) cufftDestroy(c->plan_fwd);
   dfree(c->d_x); dfree(c->d_work); dfree(c->d_yhat); dfree(c->d_samp_pos); dfree(c->d_samp_off);
   dfree(c->d_ph_ksp); dfree(c->d_ph_img); dfree(c->d_S); dfree(c->d_partials); dfree(c->d_hist); dfree(c->d_iter);
-  dfree(c->d_block_stat); dfree(c->d_wavelet_work); dfree(c->d_fft_work);
+  dfree(c->d_block_stat); dfree(c->d_fb); dfree(c->d_wavelet_work); dfree(c->d_fft_work);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return LLR_OK;

@@ -344,15 +344,25 @@ static int g_batch_eig_solver = 0;
 
 static int batch_prox(int m, int n, int mode, int rank, float lam, int batch, llr_cf32* d, void* stream) {
   if (!d || m < 1 || n < 1 || batch < 0) return set_error(LLR_ERR_INVALID, "bad matrix batch arguments");
+  if (batch == 0) return LLR_OK;
+  cudaStream_t s = (cudaStream_t)stream;
   BlockSource src;
   memset(&src, 0, sizeof(src));
   src.kind = 0;
   src.data = (float2*)d;
   src.nblocks = batch;
   ProxOp op;
+  memset(&op, 0, sizeof(op));
   op.m = m; op.n = n; op.mode = mode; op.rank = rank; op.lambda = lam; op.block_stat = nullptr;
   op.eig_solver = g_batch_eig_solver;
-  return launch_llr_prox(src, op, (cudaStream_t)stream);
+  int* fb = nullptr;
+  LLR_CUDA_TRY(cudaMallocAsync((void**)&fb, sizeof(int) * ((size_t)batch + 1), s));
+  op.fb_list = fb;
+  op.fb_count = fb + batch;
+  int st = launch_llr_prox(src, op, s);
+  cudaError_t e = cudaFreeAsync(fb, s);
+  if (st == LLR_OK && e != cudaSuccess) st = cuda_error(e, "cudaFreeAsync", __FILE__, __LINE__);
+  return st;
 }
 
 int llr_low_rank_batch_dev(int32_t m, int32_t n, int32_t rank, int32_t batch, llr_cf32* d, void* stream) {

@@ -28,6 +28,9 @@ struct BlockSource {
   PhaseTab ph;         // phase tables (null members: identity)
   int store_phase;     // 1: stored value = value * phase; 0: stored value = value
   float store_scale;   // stored value additionally scaled by this factor
+  int ph_uniform;      // every volume has the same phase tables (per-row phase suffices)
+  const int* blk_list; // optional list of block indices (with blk_count) instead of 0..nblocks-1
+  const int* blk_count;
 };
 
 struct ProxOp {
@@ -37,6 +40,8 @@ struct ProxOp {
   float lambda;
   float* block_stat;   // when non-null: write the largest Gram eigenvalue, skip the update
   int eig_solver;      // 0: tridiagonal + bisection + inverse iteration; 1: Jacobi
+  int* fb_list;        // blocks handed to the Jacobi kernel (capacity nblocks)
+  int* fb_count;
 };
 
 int launch_llr_prox(const BlockSource& src, const ProxOp& op, cudaStream_t stream);
@@ -114,6 +119,8 @@ struct llr_ctx {
   long long* d_iter;
   long long h_iter;         // host mirror (valid after sync)
   float* d_block_stat;
+  int* d_fb;                // Jacobi fallback block list (nblocks) + count
+  int ph_uniform;           // all volumes share the image-domain phase tables
   float2* d_wavelet_work;
   size_t wavelet_work_elems;
   llr::WaveletPlan wplan;

@@ -1,0 +1,685 @@
+// Fused locally-low-rank proximal step, tridiagonal eigen path (the default solver).
+//
+// One CTA owns one Casorati matrix at a time (persistent grid, two CTAs per SM):
+//   row tables (periodic wrap, block.rs:122-133 and :20-22; per-row phase)
+//   Gram G = C^H C over row chunks staged in shared memory, tiles accumulated in registers
+//   Householder tridiagonalisation, Sturm multisection for the kept eigenvalues only,
+//   inverse iteration, modified Gram-Schmidt + residual check, back-transformation
+//   C' = (C V_a) g V_a^H, one thread per row, read from and written to global memory
+// This replaces, per block, lift_data_set (block.rs:147-164), cusolver gesvda
+// (cusolver.rs:20-151), rhsCdgmmBatched (kernels.cu:11-67), the CGEMM (U S) V^H
+// (low_rank.rs:55) and un_lift_data_set (block.rs:166-184), since U_r S_r V_r^H = C V_r V_r^H.
+// Blocks keeping more than kRaMax components, or whose eigenvectors fail the residual check,
+// are appended to a device list and finished by the Jacobi kernel (llr_prox.cu).
+#include <cstdio>
+#include <algorithm>
+
+#include "llr_prox_common.cuh"
+
+namespace llr {
+
+int launch_llr_prox_jacobi(const BlockSource& src, const ProxOp& op, cudaStream_t stream);
+bool llr_prox_jacobi_supported(int m, int n);
+
+namespace {
+
+constexpr int kRaMax = 16;   // kept components handled by the tridiagonal path
+
+// Tridiagonal-path scratch (NPMAX-sized vectors and the real eigenvectors of T').
+template <int NPMAX>
+struct TrdSmem {
+  float2 u[NPMAX];      // current Householder vector
+  float2 p[NPMAX];      // tau * A22 u
+  float2 e[NPMAX];      // complex sub-diagonal of T
+  float2 delta[NPMAX];  // unitary diagonal making T' = D^H T D real
+  float d[NPMAX];       // diagonal of T
+  float ae[NPMAX];      // |e|
+  float e2[NPMAX];      // |e|^2
+  float tau[NPMAX];     // reflector scalars
+  float lam[kRaMax];    // kept eigenvalues (ascending), separated for inverse iteration
+  float Y[NPMAX * kRaMax];  // eigenvectors of T', column a at Y[a * NPMAX]
+};
+
+// =======================================================================================
+// Tridiagonal eigen path.  Householder reduction of the Hermitian Gram matrix to
+// tridiagonal T (H = I - tau u u^H, tau real), a unitary diagonal D making T' = D^H T D
+// real, Sturm-count multisection for only the eigenvalues that the singular-value map keeps
+// (above lambda^2, or the top `rank`), inverse iteration for their eigenvectors, modified
+// Gram-Schmidt plus a residual check, and back-transformation V = Q D Y.  About n^3 complex
+// flops in total against sweeps * 8 n^3 for Jacobi; blocks whose eigenvectors fail the
+// residual check take the Jacobi path.
+// =======================================================================================
+template <int NPMAX>
+__device__ void hermitian_tridiag(float2* A, int n, TrdSmem<NPMAX>* T, float* red) {
+  constexpr int lda = NPMAX + 1;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nwarps = blockDim.x >> 5;
+  for (int k = 0; k + 2 < n; ++k) {
+    const int L = n - k - 1;
+    if (warp == 0) {
+      const int i0 = lane, i1 = lane + 32;
+      float2 x0 = make_float2(0.f, 0.f), x1 = make_float2(0.f, 0.f);
+      if (i0 < L) x0 = A[(k + 1 + i0) * lda + k];
+      if (i1 < L) x1 = A[(k + 1 + i1) * lda + k];
+      float s2 = cabs2(x0) + cabs2(x1);
+      for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+      const float ax = __shfl_sync(0xffffffffu, x0.x, 0), ay = __shfl_sync(0xffffffffu, x0.y, 0);
+      const float xn = sqrtf(s2);
+      const float aa = sqrtf(ax * ax + ay * ay);
+      const float phx = aa > 0.f ? ax / aa : 1.f, phy = aa > 0.f ? ay / aa : 0.f;
+      const float2 u0 = make_float2(ax + phx * xn, ay + phy * xn);
+      const float un2 = s2 - aa * aa + cabs2(u0);
+      const float t = (xn > 0.f && un2 > 0.f) ? 2.f / un2 : 0.f;
+      if (lane == 0) {
+        T->tau[k] = t;
+        T->e[k] = make_float2(-phx * xn, -phy * xn);
+        A[(k + 1) * lda + k] = u0;  // column k now stores u_k for the back-transformation
+      }
+      if (i0 < L) T->u[i0] = (i0 == 0) ? u0 : x0;
+      if (i1 < L) T->u[i1] = x1;
+    }
+    __syncthreads();
+    const float t = T->tau[k];
+    if (t != 0.f) {
+      // p = t * A22 u : four threads per row
+      const int row = tid >> 2, part = tid & 3;
+      float2 acc = make_float2(0.f, 0.f);
+      if (row < L) {
+        const float2* Ar = A + (k + 1 + row) * lda + (k + 1);
+        for (int j = part; j < L; j += 4) cfma(acc, Ar[j], T->u[j]);
+      }
+      acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 1);
+      acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 1);
+      acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 2);
+      acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 2);
+      float dp = 0.f;
+      if (row < L && part == 0) {
+        const float2 pv = cscale(acc, t);
+        T->p[row] = pv;
+        const float2 uv = T->u[row];
+        dp = uv.x * pv.x + uv.y * pv.y;  // Re(conj(u) p)
+      }
+      for (int o = 16; o > 0; o >>= 1) dp += __shfl_xor_sync(0xffffffffu, dp, o);
+      if (lane == 0) red[warp] = dp;
+      __syncthreads();
+      float up = 0.f;
+      for (int w = 0; w < nwarps; ++w) up += red[w];
+      const float K = 0.5f * t * up;
+      // A22 -= u w^H + w u^H,  w = p - K u
+      const int tj = tid & 15, ti = tid >> 4;
+      for (int i = ti; i < L; i += 16) {
+        const float2 ui = T->u[i];
+        const float2 wi = csub(T->p[i], cscale(ui, K));
+        float2* Ar = A + (k + 1 + i) * lda + (k + 1);
+        for (int j = tj; j < L; j += 16) {
+          const float2 uj = T->u[j];
+          const float2 wj = csub(T->p[j], cscale(uj, K));
+          Ar[j] = csub(csub(Ar[j], cmul_bc(ui, wj)), cmul_bc(wi, uj));
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (tid < n) T->d[tid] = A[tid * lda + tid].x;
+  if (tid == 0) {
+    if (n >= 2) T->e[n - 2] = A[(n - 1) * lda + n - 2];
+    for (int k = n - 2; k < n; ++k)
+      if (k >= 0) T->tau[k] = 0.f;
+  }
+  __syncthreads();
+}
+
+// Sturm count: number of eigenvalues of the real tridiagonal (d, e2 = offdiag^2) below x.
+__device__ __forceinline__ int sturm_count(const float* d, const float* e2, int n, float x, float pivmin) {
+  float q = d[0] - x;
+  if (fabsf(q) <= pivmin) q = -pivmin;
+  int c = q < 0.f;
+  for (int i = 1; i < n; ++i) {
+    q = d[i] - x - e2[i - 1] * __frcp_rn(q);
+    if (fabsf(q) <= pivmin) q = -pivmin;
+    c += q < 0.f;
+  }
+  return c;
+}
+
+// Real form T' (D), Gershgorin interval, and the active index range (eigenvalues
+// n_below .. n_below + ra - 1 in ascending order).
+template <int NPMAX>
+__device__ void tridiag_setup(TrdSmem<NPMAX>* T, int n, int mode, int rank, float lam, Misc* misc) {
+  if (threadIdx.x == 0) {
+    float2 dl = make_float2(1.f, 0.f);
+    float e2max = 0.f;
+    for (int k = 0; k < n; ++k) {
+      T->delta[k] = dl;
+      if (k + 1 < n) {
+        const float2 ek = T->e[k];
+        const float a = sqrtf(cabs2(ek));
+        T->ae[k] = a;
+        T->e2[k] = a * a;
+        e2max = fmaxf(e2max, a * a);
+        if (a > 0.f) dl = cmul(dl, make_float2(ek.x / a, ek.y / a));
+      } else {
+        T->ae[k] = 0.f;
+        T->e2[k] = 0.f;
+      }
+    }
+    float gl = 3.0e38f, gu = -3.0e38f;
+    for (int k = 0; k < n; ++k) {
+      const float r = (k > 0 ? T->ae[k - 1] : 0.f) + (k + 1 < n ? T->ae[k] : 0.f);
+      gl = fminf(gl, T->d[k] - r);
+      gu = fmaxf(gu, T->d[k] + r);
+    }
+    const float tn = fmaxf(fabsf(gl), fabsf(gu));
+    gl -= 4.f * 1.1920929e-7f * tn * n + 1e-30f;
+    gu += 4.f * 1.1920929e-7f * tn * n + 1e-30f;
+    misc->gl = gl;
+    misc->gu = gu;
+    misc->tnorm = tn;
+    misc->pivmin = 1.1754944e-38f * fmaxf(1.f, e2max);
+    int nb;
+    if (mode == LLR_PROX_HARD_RANK) nb = max(0, n - rank);
+    else if (!(lam > 0.f)) nb = 0;
+    else nb = sturm_count(T->d, T->e2, n, lam * lam, misc->pivmin);
+    misc->n_below = nb;
+    misc->ra = n - nb;
+    misc->fail = 0;
+  }
+  __syncthreads();
+}
+
+// Multisection: a group of G lanes (G = 32, 16 or 8 by the number of eigenvalues) refines
+// eigenvalue j by (G+1)-way splits of its Gershgorin interval; warp-uniform loop.
+template <int NPMAX>
+__device__ void tridiag_eigenvalues(TrdSmem<NPMAX>* T, int n, int j0, int count, const Misc* misc) {
+  const int lane = threadIdx.x & 31;
+  const int G = count <= (int)(blockDim.x >> 5) ? 32 : (count <= (int)(blockDim.x >> 4) ? 16 : 8);
+  const int gl = lane & (G - 1);
+  const int group = threadIdx.x / G;
+  const int ngroups = blockDim.x / G;
+  const unsigned gmask = G == 32 ? 0xffffffffu : ((1u << G) - 1u);
+  const float inv = 1.f / (float)(G + 1);
+  for (int base = 0; base < count; base += ngroups) {
+    const int a = base + group;
+    const bool act = a < count;
+    const int j = j0 + (act ? a : 0);
+    float lo = misc->gl, hi = misc->gu;
+    for (int round = 0; round < 24; ++round) {
+      const bool conv = !act || (hi - lo) <= 2.4e-7f * fmaxf(fabsf(lo), fabsf(hi)) + misc->pivmin;
+      if (__all_sync(0xffffffffu, conv)) break;
+      const float x = lo + (hi - lo) * (float)(gl + 1) * inv;
+      const bool le = act ? (sturm_count(T->d, T->e2, n, x, misc->pivmin) <= j) : true;
+      const unsigned bal = __ballot_sync(0xffffffffu, le);
+      const int nt = __popc((bal >> (lane & ~(G - 1) & 31)) & gmask);
+      const float nlo = nt > 0 ? lo + (hi - lo) * (float)nt * inv : lo;
+      const float nhi = nt < G ? lo + (hi - lo) * (float)(nt + 1) * inv : hi;
+      lo = nlo;
+      hi = nhi;
+    }
+    if (act && gl == 0) T->lam[a] = 0.5f * (lo + hi);
+  }
+  __syncthreads();
+}
+
+// Inverse iteration (one thread per active eigenvalue) on T' - lambda I with partial
+// pivoting; three solves from a deterministic start vector.
+template <int NPMAX>
+__device__ void tridiag_vectors(TrdSmem<NPMAX>* T, int n, int ra, Misc* misc) {
+  const float eps = 1.1920929e-7f;
+  const float tiny = eps * fmaxf(misc->tnorm, 1e-30f);
+  if (threadIdx.x == 0) {  // separate (near-)equal eigenvalues (LAPACK stein convention)
+    const float sep = 10.f * eps * fmaxf(misc->tnorm, 1e-30f);
+    for (int a = 1; a < ra; ++a)
+      if (T->lam[a] - T->lam[a - 1] < sep) T->lam[a] = T->lam[a - 1] + sep;
+  }
+  __syncthreads();
+  for (int a = threadIdx.x; a < ra; a += blockDim.x) {
+    const float lam = T->lam[a];
+    float dd[NPMAX], du[NPMAX], du2[NPMAX], dl[NPMAX], b[NPMAX];
+    unsigned long long piv = 0ull;
+    for (int i = 0; i < n; ++i) {
+      dd[i] = T->d[i] - lam;
+      du[i] = (i + 1 < n) ? T->ae[i] : 0.f;
+      dl[i] = du[i];
+      du2[i] = 0.f;
+    }
+    for (int i = 0; i + 1 < n; ++i) {
+      if (fabsf(dd[i]) >= fabsf(dl[i])) {
+        if (fabsf(dd[i]) < tiny) dd[i] = copysignf(tiny, dd[i] == 0.f ? 1.f : dd[i]);
+        const float f = dl[i] * __frcp_rn(dd[i]);
+        dl[i] = f;
+        dd[i + 1] -= f * du[i];
+      } else {
+        const float f = dd[i] * __frcp_rn(dl[i]);
+        dd[i] = dl[i];
+        dl[i] = f;
+        const float tmp = du[i];
+        du[i] = dd[i + 1];
+        dd[i + 1] = tmp - f * dd[i + 1];
+        if (i + 2 < n) {
+          du2[i] = du[i + 1];
+          du[i + 1] = -f * du[i + 1];
+        }
+        piv |= (1ull << i);
+      }
+    }
+    if (fabsf(dd[n - 1]) < tiny) dd[n - 1] = copysignf(tiny, dd[n - 1] == 0.f ? 1.f : dd[n - 1]);
+    for (int i = 0; i < n; ++i) dd[i] = __frcp_rn(dd[i]);  // keep reciprocals of the pivots
+    uint64_t h = llr_splitmix64(0x1234567ull + (uint64_t)a);
+    for (int i = 0; i < n; ++i) {
+      h = llr_splitmix64(h);
+      b[i] = (float)((h >> 40) & 0xffffff) * (1.f / 16777216.f) - 0.5f;
+    }
+    for (int it = 0; it < 3; ++it) {
+      for (int i = 0; i + 1 < n; ++i) {
+        if (piv & (1ull << i)) {
+          const float t = b[i];
+          b[i] = b[i + 1];
+          b[i + 1] = t - dl[i] * b[i];
+        } else {
+          b[i + 1] -= dl[i] * b[i];
+        }
+      }
+      b[n - 1] *= dd[n - 1];
+      if (n >= 2) b[n - 2] = (b[n - 2] - du[n - 2] * b[n - 1]) * dd[n - 2];
+      for (int i = n - 3; i >= 0; --i) b[i] = (b[i] - du[i] * b[i + 1] - du2[i] * b[i + 2]) * dd[i];
+      float mx = 0.f;
+      for (int i = 0; i < n; ++i) mx = fmaxf(mx, fabsf(b[i]));
+      const float sc = mx > 0.f ? 1.f / mx : 1.f;
+      for (int i = 0; i < n; ++i) b[i] *= sc;
+    }
+    for (int i = 0; i < n; ++i) T->Y[a * NPMAX + i] = b[i];
+  }
+  __syncthreads();
+  // modified Gram-Schmidt over the active vectors + residual check (warp 0)
+  if ((threadIdx.x >> 5) == 0) {
+    const int lane = threadIdx.x & 31;
+    const float tol = 2e-5f * fmaxf(misc->tnorm, 1e-30f);
+    int bad = 0;
+    for (int a = 0; a < ra; ++a) {
+      float* y = T->Y + a * NPMAX;
+      float y0 = lane < n ? y[lane] : 0.f, y1 = lane + 32 < n ? y[lane + 32] : 0.f;
+      for (int c = 0; c < a; ++c) {
+        const float* z = T->Y + c * NPMAX;
+        const float z0 = lane < n ? z[lane] : 0.f, z1 = lane + 32 < n ? z[lane + 32] : 0.f;
+        float dp = y0 * z0 + y1 * z1;
+        for (int o = 16; o > 0; o >>= 1) dp += __shfl_xor_sync(0xffffffffu, dp, o);
+        y0 -= dp * z0;
+        y1 -= dp * z1;
+      }
+      float nn = y0 * y0 + y1 * y1;
+      for (int o = 16; o > 0; o >>= 1) nn += __shfl_xor_sync(0xffffffffu, nn, o);
+      const float inv = nn > 0.f ? rsqrtf(nn) : 0.f;
+      y0 *= inv;
+      y1 *= inv;
+      if (lane < n) y[lane] = y0;
+      if (lane + 32 < n) y[lane + 32] = y1;
+      __syncwarp();
+      // residual |T' y - lambda y|
+      const float lam = T->lam[a];
+      float r2 = 0.f;
+      for (int h = 0; h < 2; ++h) {
+        const int i = lane + 32 * h;
+        if (i < n) {
+          float r = (T->d[i] - lam) * y[i];
+          if (i > 0) r += T->ae[i - 1] * y[i - 1];
+          if (i + 1 < n) r += T->ae[i] * y[i + 1];
+          r2 += r * r;
+        }
+      }
+      for (int o = 16; o > 0; o >>= 1) r2 += __shfl_xor_sync(0xffffffffu, r2, o);
+      if (!(nn > 0.f) || !(sqrtf(r2) <= tol)) bad = 1;
+      __syncwarp();
+    }
+    if (lane == 0) misc->fail = bad;
+  }
+  __syncthreads();
+}
+
+// Va[i * kRaMax + a] = (Q D y_a)_i (complex), one warp per vector.
+template <int NPMAX>
+__device__ void tridiag_backtransform(const float2* A, TrdSmem<NPMAX>* T, float2* V, int n, int ra) {
+  constexpr int lda = NPMAX + 1;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int a = warp; a < ra; a += nw) {
+    const float* y = T->Y + a * NPMAX;
+    float2 v0 = make_float2(0.f, 0.f), v1 = make_float2(0.f, 0.f);
+    const int i0 = lane, i1 = lane + 32;
+    if (i0 < n) v0 = cscale(T->delta[i0], y[i0]);
+    if (i1 < n) v1 = cscale(T->delta[i1], y[i1]);
+    for (int k = n - 3; k >= 0; --k) {
+      const float t = T->tau[k];
+      if (t == 0.f) continue;
+      // u_k lives in column k of A below the diagonal (rows k+1 .. n-1), with u_k[0] at row k+1
+      // replaced by the value kept in column k during the reduction.
+      const float2 u0 = (i0 > k && i0 < n) ? A[i0 * lda + k] : make_float2(0.f, 0.f);
+      const float2 u1 = (i1 > k && i1 < n) ? A[i1 * lda + k] : make_float2(0.f, 0.f);
+      float2 s = cadd(cmulc(u0, v0), cmulc(u1, v1));
+      for (int o = 16; o > 0; o >>= 1) {
+        s.x += __shfl_xor_sync(0xffffffffu, s.x, o);
+        s.y += __shfl_xor_sync(0xffffffffu, s.y, o);
+      }
+      s = cscale(s, t);
+      v0 = csub(v0, cmul(u0, s));
+      v1 = csub(v1, cmul(u1, s));
+    }
+    if (i0 < n) V[i0 * kRaMax + a] = v0;
+    if (i1 < n) V[i1 * kRaMax + a] = v1;
+  }
+  __syncthreads();
+}
+
+
+// ---------------------------------------------------------------------------------------
+// Per-block row tables: element (r, q) of the Casorati matrix lives at off[r] + q * qstride,
+// and (for per-row uniform phase) carries phase ph[r].
+// ---------------------------------------------------------------------------------------
+struct RowTab {
+  int off;   // planar offset of the voxel (volume 0) or row index (matrix batches)
+  int cx;    // x coordinate
+  int cyz;   // y | z << 16
+  int pad;
+};
+
+__device__ __forceinline__ float2 load_elem(const BlockSource& s, long long base, const RowTab& rt, const float2* rowph,
+                                            int r, int q, long long qstride) {
+  float2 v = s.data[base + (long long)rt.off + (long long)q * qstride];
+  if (s.kind == 1) {
+    float2 p;
+    if (s.ph_uniform) p = rowph[r];
+    else p = phase_at(s.ph, s.g, q, rt.cx, rt.cyz & 0xffff, rt.cyz >> 16);
+    v = cscale(cmul_bc(v, p), s.load_scale);
+  }
+  return v;
+}
+
+__device__ __forceinline__ void store_elem(const BlockSource& s, long long base, const RowTab& rt, const float2* rowph,
+                                           int r, int q, long long qstride, float2 v) {
+  if (s.kind == 1) {
+    v = cscale(v, s.store_scale);
+    if (s.store_phase) {
+      float2 p;
+      if (s.ph_uniform) p = rowph[r];
+      else p = phase_at(s.ph, s.g, q, rt.cx, rt.cyz & 0xffff, rt.cyz >> 16);
+      v = cmul(v, p);
+    }
+  }
+  s.data[base + (long long)rt.off + (long long)q * qstride] = v;
+}
+
+struct TrdLayout {
+  int rc;        // rows per staged chunk
+  int ldch;      // leading dimension of a staged chunk (odd)
+  int np, ksplit;
+  size_t off_row, off_rowph, off_A, off_C, off_trd, off_V, off_g, total;
+};
+
+template <int NPMAX, int TG>
+TrdLayout make_trd_layout(int m, int n) {
+  TrdLayout L;
+  const int nt = (n + TG - 1) / TG;
+  L.np = nt * TG;
+  L.ksplit = std::max(1, kLlrThreads / (nt * nt));
+  int rc = (40 * 1024) / (8 * n);
+  rc = std::max(32, std::min(rc, 256));
+  L.rc = std::min(rc, m);
+  L.ldch = (L.rc & 1) ? L.rc : L.rc + 1;
+  size_t off = 256;
+  L.off_row = off; off = align16(off + sizeof(RowTab) * (size_t)m);
+  L.off_rowph = off; off = align16(off + sizeof(float2) * (size_t)m);
+  L.off_A = off; off = align16(off + sizeof(float2) * NPMAX * (NPMAX + 1));
+  L.off_C = off;
+  const size_t chunk = sizeof(float2) * (size_t)n * L.ldch;
+  const size_t scr = L.ksplit > 1 ? sizeof(float2) * (size_t)L.ksplit * L.np * L.np : 0;
+  off = align16(off + std::max(chunk, scr));
+  L.off_trd = off; off = align16(off + sizeof(TrdSmem<NPMAX>));
+  L.off_V = off; off = align16(off + sizeof(float2) * NPMAX * kRaMax);
+  L.off_g = off; off = align16(off + sizeof(float) * kRaMax);
+  L.total = off;
+  return L;
+}
+
+template <int RM>
+__device__ void apply_rows(const BlockSource& s, long long base, const RowTab* rows, const float2* rowph, int m, int n,
+                           long long qstride, const float2* Va, const float* g, int ra) {
+  for (int r = threadIdx.x; r < m; r += blockDim.x) {
+    const RowTab rt = rows[r];
+    float2 t[RM];
+#pragma unroll
+    for (int a = 0; a < RM; ++a) t[a] = make_float2(0.f, 0.f);
+    for (int k = 0; k < n; ++k) {
+      const float2 c = load_elem(s, base, rt, rowph, r, k, qstride);
+#pragma unroll
+      for (int a = 0; a < RM; ++a)
+        if (a < ra) cfma(t[a], c, Va[k * kRaMax + a]);
+    }
+#pragma unroll
+    for (int a = 0; a < RM; ++a)
+      if (a < ra) t[a] = cscale(t[a], g[a]);
+    for (int q = 0; q < n; ++q) {
+      float2 c = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int a = 0; a < RM; ++a)
+        if (a < ra) cfma_cb(c, t[a], Va[q * kRaMax + a]);
+      store_elem(s, base, rt, rowph, r, q, qstride, c);
+    }
+  }
+}
+
+template <int NPMAX, int TG>
+__global__ void __launch_bounds__(kLlrThreads, 2) llr_prox_trd_kernel(BlockSource src, ProxOp op, TrdLayout L) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  Misc* misc = reinterpret_cast<Misc*>(smem);
+  RowTab* rows = reinterpret_cast<RowTab*>(smem + L.off_row);
+  float2* rowph = reinterpret_cast<float2*>(smem + L.off_rowph);
+  float2* A = reinterpret_cast<float2*>(smem + L.off_A);
+  float2* Cch = reinterpret_cast<float2*>(smem + L.off_C);
+  TrdSmem<NPMAX>* trd = reinterpret_cast<TrdSmem<NPMAX>*>(smem + L.off_trd);
+  float2* Va = reinterpret_cast<float2*>(smem + L.off_V);
+  float* g = reinterpret_cast<float*>(smem + L.off_g);
+  constexpr int lda = NPMAX + 1;
+  const int m = op.m, n = op.n, tid = threadIdx.x;
+  const long long qstride = src.kind == 1 ? src.g.V : (long long)m;
+
+  if (tid == 0) block_shift(src, misc->shift);
+  __syncthreads();
+  const int sh[3] = {misc->shift[0], misc->shift[1], misc->shift[2]};
+
+  for (long long blk = blockIdx.x; blk < src.nblocks; blk += gridDim.x) {
+    const long long base = src.kind == 1 ? 0 : blk * (long long)m * n;
+    // row tables
+    for (int r = tid; r < m; r += blockDim.x) {
+      RowTab rt;
+      if (src.kind == 1) {
+        int ix, iy, iz;
+        block_row_coord(src, blk, sh, r, ix, iy, iz);
+        rt.off = (int)planar_index(src.g, ix, iy, iz, 0);
+        rt.cx = ix;
+        rt.cyz = iy | (iz << 16);
+        if (src.ph_uniform) rowph[r] = phase_at(src.ph, src.g, 0, ix, iy, iz);
+      } else {
+        rt.off = r;
+        rt.cx = 0;
+        rt.cyz = 0;
+      }
+      rt.pad = 0;
+      rows[r] = rt;
+    }
+    // Gram over staged row chunks; tile accumulators stay in registers
+    const int nt = (n + TG - 1) / TG;
+    const int tiles = nt * nt;
+    const bool gram_thread = tid < tiles * L.ksplit;
+    const int tile = tid % tiles, ks = tid / tiles;
+    const int ti = tile / nt, tj = tile - ti * nt;
+    float2 acc[TG][TG];
+#pragma unroll
+    for (int a = 0; a < TG; ++a)
+#pragma unroll
+      for (int b = 0; b < TG; ++b) acc[a][b] = make_float2(0.f, 0.f);
+    __syncthreads();
+    for (int c0 = 0; c0 < m; c0 += L.rc) {
+      const int rc = min(L.rc, m - c0);
+      {
+        const int tot = rc * n;
+        int q = tid / rc, rr = tid - (tid / rc) * rc;
+        const int sq = blockDim.x / rc, sr = blockDim.x - sq * rc;
+        for (int i = tid; i < tot; i += blockDim.x) {
+          const int r = c0 + rr;
+          Cch[q * L.ldch + rr] = load_elem(src, base, rows[r], rowph, r, q, qstride);
+          rr += sr;
+          q += sq;
+          if (rr >= rc) { rr -= rc; ++q; }
+        }
+      }
+      __syncthreads();
+      if (gram_thread) {
+        const int r0 = (int)(((long long)rc * ks) / L.ksplit), r1 = (int)(((long long)rc * (ks + 1)) / L.ksplit);
+        for (int r = r0; r < r1; ++r) {
+          float2 ci[TG], cj[TG];
+#pragma unroll
+          for (int a = 0; a < TG; ++a) {
+            const int cI = ti + nt * a, cJ = tj + nt * a;
+            ci[a] = cI < n ? Cch[cI * L.ldch + r] : make_float2(0.f, 0.f);
+            cj[a] = cJ < n ? Cch[cJ * L.ldch + r] : make_float2(0.f, 0.f);
+          }
+#pragma unroll
+          for (int a = 0; a < TG; ++a)
+#pragma unroll
+            for (int b = 0; b < TG; ++b) cfma_ca(acc[a][b], ci[a], cj[b]);
+        }
+      }
+      __syncthreads();
+    }
+    if (L.ksplit == 1) {
+      if (gram_thread) {
+#pragma unroll
+        for (int a = 0; a < TG; ++a)
+#pragma unroll
+          for (int b = 0; b < TG; ++b) {
+            const int cI = ti + nt * a, cJ = tj + nt * b;
+            if (cI < n && cJ < n) A[cI * lda + cJ] = acc[a][b];
+          }
+      }
+    } else {
+      float2* P = Cch;  // chunk buffer is free now
+      if (gram_thread) {
+#pragma unroll
+        for (int a = 0; a < TG; ++a)
+#pragma unroll
+          for (int b = 0; b < TG; ++b)
+            P[(size_t)ks * L.np * L.np + (ti + nt * a) * L.np + (tj + nt * b)] = acc[a][b];
+      }
+      __syncthreads();
+      for (int idx = tid; idx < n * n; idx += blockDim.x) {
+        const int i = idx / n, j = idx - i * n;
+        float2 sacc = make_float2(0.f, 0.f);
+        for (int k = 0; k < L.ksplit; ++k) sacc = cadd(sacc, P[(size_t)k * L.np * L.np + i * L.np + j]);
+        A[i * lda + j] = sacc;
+      }
+    }
+    __syncthreads();
+
+    hermitian_tridiag<NPMAX>(A, n, trd, misc->red);
+    if (op.block_stat) {
+      tridiag_setup<NPMAX>(trd, n, LLR_PROX_HARD_RANK, 1, 0.f, misc);
+      tridiag_eigenvalues<NPMAX>(trd, n, n - 1, 1, misc);
+      if (tid == 0) op.block_stat[blk] = trd->lam[0];
+      __syncthreads();
+      continue;
+    }
+    tridiag_setup<NPMAX>(trd, n, op.mode, op.rank, op.lambda, misc);
+    const int ra = misc->ra, nb = misc->n_below;
+    if (ra == n && op.mode == LLR_PROX_HARD_RANK) {
+      __syncthreads();
+      continue;  // rank >= n: identity, nothing to write
+    }
+    if (ra == 0) {
+      for (int idx = tid; idx < m * n; idx += blockDim.x) {
+        const int q = idx / m, r = idx - q * m;
+        store_elem(src, base, rows[r], rowph, r, q, qstride, make_float2(0.f, 0.f));
+      }
+      __syncthreads();
+      continue;
+    }
+    bool fallback = ra > kRaMax;
+    if (!fallback) {
+      tridiag_eigenvalues<NPMAX>(trd, n, nb, ra, misc);
+      tridiag_vectors<NPMAX>(trd, n, ra, misc);
+      fallback = misc->fail != 0;
+    }
+    if (fallback) {
+      if (tid == 0 && op.fb_list) {
+        const int pos = atomicAdd(op.fb_count, 1);
+        op.fb_list[pos] = (int)blk;
+      }
+      __syncthreads();
+      continue;
+    }
+    tridiag_backtransform<NPMAX>(A, trd, Va, n, ra);
+    if (tid < ra) {
+      float gv = 1.f;
+      if (op.mode != LLR_PROX_HARD_RANK) {
+        const float sv = sqrtf(fmaxf(trd->lam[tid], 0.f));
+        gv = (sv > op.lambda) ? (1.f - op.lambda / sv) : 0.f;
+      }
+      g[tid] = gv;
+    }
+    __syncthreads();
+    if (ra <= 4) apply_rows<4>(src, base, rows, rowph, m, n, qstride, Va, g, ra);
+    else if (ra <= 8) apply_rows<8>(src, base, rows, rowph, m, n, qstride, Va, g, ra);
+    else apply_rows<kRaMax>(src, base, rows, rowph, m, n, qstride, Va, g, ra);
+    __syncthreads();
+  }
+}
+
+template <int NPMAX, int TG>
+int launch_trd_instance(const BlockSource& src, const ProxOp& op, cudaStream_t stream) {
+  TrdLayout L = make_trd_layout<NPMAX, TG>(op.m, op.n);
+  if (L.total > 227 * 1024)
+    return set_error(LLR_ERR_UNSUPPORTED, "Casorati %dx%d needs %zu B of shared memory", op.m, op.n, L.total);
+  auto kern = llr_prox_trd_kernel<NPMAX, TG>;
+  LLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total));
+  int dev = 0, nsm = 0, occ = 0;
+  LLR_CUDA_TRY(cudaGetDevice(&dev));
+  LLR_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  LLR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kLlrThreads, L.total));
+  if (occ < 1) return set_error(LLR_ERR_UNSUPPORTED, "prox kernel cannot be resident (smem %zu B)", L.total);
+  const long long grid = std::min<long long>(src.nblocks, (long long)nsm * occ);
+  if (grid < 1) return LLR_OK;
+  kern<<<(unsigned)grid, kLlrThreads, L.total, stream>>>(src, op, L);
+  LLR_CUDA_TRY(cudaGetLastError());
+  return LLR_OK;
+}
+
+}  // namespace
+
+bool llr_prox_supported(int m, int n) {
+  if (m < 1 || n < 1 || n > 64 || m > 65535) return false;
+  size_t t;
+  if (n <= 16) t = make_trd_layout<16, 2>(m, n).total;
+  else if (n <= 32) t = make_trd_layout<32, 2>(m, n).total;
+  else t = make_trd_layout<64, 4>(m, n).total;
+  return t <= 227 * 1024 && llr_prox_jacobi_supported(m, n);
+}
+
+// Tridiagonal-path prox over every block, then the Jacobi kernel over the blocks it handed
+// back (more than kRaMax kept components, or eigenvectors failing the residual check).
+int launch_llr_prox(const BlockSource& src, const ProxOp& op, cudaStream_t stream) {
+  if (op.n < 1 || op.m < 1) return set_error(LLR_ERR_INVALID, "empty Casorati matrix %dx%d", op.m, op.n);
+  if (src.nblocks == 0) return LLR_OK;
+  if (op.eig_solver == 1) return launch_llr_prox_jacobi(src, op, stream);
+  if (!op.block_stat && !op.fb_list)
+    return set_error(LLR_ERR_INVALID, "tridiagonal prox needs a fallback block list");
+  if (op.fb_count) LLR_CUDA_TRY(cudaMemsetAsync(op.fb_count, 0, sizeof(int), stream));
+  int st;
+  if (op.n <= 16) st = launch_trd_instance<16, 2>(src, op, stream);
+  else if (op.n <= 32) st = launch_trd_instance<32, 2>(src, op, stream);
+  else if (op.n <= 64) st = launch_trd_instance<64, 4>(src, op, stream);
+  else return set_error(LLR_ERR_UNSUPPORTED, "Casorati column count %d > 64 is not supported", op.n);
+  if (st != LLR_OK || op.block_stat) return st;
+  BlockSource fb = src;
+  fb.blk_list = op.fb_list;
+  fb.blk_count = op.fb_count;
+  return launch_llr_prox_jacobi(fb, op, stream);
+}
+
+}  // namespace llr
