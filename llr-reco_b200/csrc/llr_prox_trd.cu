@@ -28,7 +28,7 @@ constexpr int kRaMax = 16;   // kept components handled by the tridiagonal path
 // Tridiagonal-path scratch (NPMAX-sized vectors and the real eigenvectors of T').
 template <int NPMAX>
 struct TrdSmem {
-  float2 u[NPMAX];      // current Householder vector
+  float2 u[2][NPMAX];   // Householder vector of the current step and x of the next one
   float2 p[NPMAX];      // tau * A22 u
   float2 e[NPMAX];      // complex sub-diagonal of T
   float2 delta[NPMAX];  // unitary diagonal making T' = D^H T D real
@@ -36,57 +36,77 @@ struct TrdSmem {
   float ae[NPMAX];      // |e|
   float e2[NPMAX];      // |e|^2
   float tau[NPMAX];     // reflector scalars
-  float lam[kRaMax];    // kept eigenvalues (ascending), separated for inverse iteration
+  float nrm[16];        // partial squared norms of the next column
+  float lam[kRaMax];    // kept eigenvalues (ascending), separated for the vector solve
   float Y[NPMAX * kRaMax];  // eigenvectors of T', column a at Y[a * NPMAX]
 };
 
+__device__ __forceinline__ float warp_sum(float v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
 // =======================================================================================
 // Tridiagonal eigen path.  Householder reduction of the Hermitian Gram matrix to
-// tridiagonal T (H = I - tau u u^H, tau real), a unitary diagonal D making T' = D^H T D
-// real, Sturm-count multisection for only the eigenvalues that the singular-value map keeps
-// (above lambda^2, or the top `rank`), inverse iteration for their eigenvectors, modified
-// Gram-Schmidt plus a residual check, and back-transformation V = Q D Y.  About n^3 complex
-// flops in total against sweeps * 8 n^3 for Jacobi; blocks whose eigenvectors fail the
-// residual check take the Jacobi path.
+// tridiagonal T (H = I - tau u u^H, tau real) working on the lower triangle only, a
+// unitary diagonal D making T' = D^H T D real, Sturm-count multisection for only the
+// eigenvalues that the singular-value map keeps (above lambda^2, or the top `rank`),
+// eigenvectors of T' from a twisted factorisation (stationary and progressive qd
+// recurrences, twist index at the smallest |gamma|), modified Gram-Schmidt plus a residual
+// check, and back-transformation V = Q D Y.  About n^3 complex flops in total against
+// sweeps * 8 n^3 for Jacobi; blocks whose eigenvectors fail the residual check go to the
+// Jacobi kernel.
 // =======================================================================================
 template <int NPMAX>
 __device__ void hermitian_tridiag(float2* A, int n, TrdSmem<NPMAX>* T, float* red) {
   constexpr int lda = NPMAX + 1;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nwarps = blockDim.x >> 5;
+  const int tj = tid & 15, ti = tid >> 4;
+  if (n >= 3) {  // vector and norm of column 0; later columns come from the previous update
+    if (warp == 0) {
+      float s2 = 0.f;
+      for (int i = lane; i < n - 1; i += 32) {
+        const float2 x = A[(1 + i) * lda];
+        s2 += cabs2(x);
+        T->u[0][i] = x;
+      }
+      s2 = warp_sum(s2);
+      if (lane < 16) T->nrm[lane] = lane == 0 ? s2 : 0.f;
+    }
+    __syncthreads();
+  }
   for (int k = 0; k + 2 < n; ++k) {
     const int L = n - k - 1;
-    if (warp == 0) {
-      const int i0 = lane, i1 = lane + 32;
-      float2 x0 = make_float2(0.f, 0.f), x1 = make_float2(0.f, 0.f);
-      if (i0 < L) x0 = A[(k + 1 + i0) * lda + k];
-      if (i1 < L) x1 = A[(k + 1 + i1) * lda + k];
-      float s2 = cabs2(x0) + cabs2(x1);
-      for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
-      const float ax = __shfl_sync(0xffffffffu, x0.x, 0), ay = __shfl_sync(0xffffffffu, x0.y, 0);
+    const int cur = k & 1, nxt = cur ^ 1;
+    float2* U = T->u[cur];
+    if (tid == 0) {
+      float s2 = 0.f;
+      for (int i = 0; i < 16; ++i) { s2 += T->nrm[i]; T->nrm[i] = 0.f; }
+      const float2 x0 = A[(k + 1) * lda + k];
       const float xn = sqrtf(s2);
-      const float aa = sqrtf(ax * ax + ay * ay);
-      const float phx = aa > 0.f ? ax / aa : 1.f, phy = aa > 0.f ? ay / aa : 0.f;
-      const float2 u0 = make_float2(ax + phx * xn, ay + phy * xn);
+      const float aa = sqrtf(cabs2(x0));
+      const float phx = aa > 0.f ? x0.x / aa : 1.f, phy = aa > 0.f ? x0.y / aa : 0.f;
+      const float2 u0 = make_float2(x0.x + phx * xn, x0.y + phy * xn);
       const float un2 = s2 - aa * aa + cabs2(u0);
       const float t = (xn > 0.f && un2 > 0.f) ? 2.f / un2 : 0.f;
-      if (lane == 0) {
-        T->tau[k] = t;
-        T->e[k] = make_float2(-phx * xn, -phy * xn);
-        A[(k + 1) * lda + k] = u0;  // column k now stores u_k for the back-transformation
-      }
-      if (i0 < L) T->u[i0] = (i0 == 0) ? u0 : x0;
-      if (i1 < L) T->u[i1] = x1;
+      T->tau[k] = t;
+      T->e[k] = make_float2(-phx * xn, -phy * xn);
+      A[(k + 1) * lda + k] = u0;  // column k keeps u_k for the back-transformation
+      U[0] = u0;
     }
     __syncthreads();
     const float t = T->tau[k];
+    float2* A22 = A + (k + 1) * lda + (k + 1);
     if (t != 0.f) {
-      // p = t * A22 u : four threads per row
+      // p = t * A22 u from the lower triangle (A22[i][j] = conj(A22[j][i]) for j > i)
       const int row = tid >> 2, part = tid & 3;
       float2 acc = make_float2(0.f, 0.f);
       if (row < L) {
-        const float2* Ar = A + (k + 1 + row) * lda + (k + 1);
-        for (int j = part; j < L; j += 4) cfma(acc, Ar[j], T->u[j]);
+        for (int j = part; j < L; j += 4) {
+          const float2 a = (j <= row) ? A22[row * lda + j] : cconj(A22[j * lda + row]);
+          cfma(acc, a, U[j]);
+        }
       }
       acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 1);
       acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 1);
@@ -96,26 +116,44 @@ __device__ void hermitian_tridiag(float2* A, int n, TrdSmem<NPMAX>* T, float* re
       if (row < L && part == 0) {
         const float2 pv = cscale(acc, t);
         T->p[row] = pv;
-        const float2 uv = T->u[row];
+        const float2 uv = U[row];
         dp = uv.x * pv.x + uv.y * pv.y;  // Re(conj(u) p)
       }
-      for (int o = 16; o > 0; o >>= 1) dp += __shfl_xor_sync(0xffffffffu, dp, o);
+      dp = warp_sum(dp);
       if (lane == 0) red[warp] = dp;
       __syncthreads();
       float up = 0.f;
       for (int w = 0; w < nwarps; ++w) up += red[w];
       const float K = 0.5f * t * up;
-      // A22 -= u w^H + w u^H,  w = p - K u
-      const int tj = tid & 15, ti = tid >> 4;
+      // lower-triangle update A22 -= u w^H + w u^H,  w = p - K u; the threads of column 0
+      // also hand the next step its x vector and the partial norms.
+      float nacc = 0.f;
       for (int i = ti; i < L; i += 16) {
-        const float2 ui = T->u[i];
+        const float2 ui = U[i];
         const float2 wi = csub(T->p[i], cscale(ui, K));
-        float2* Ar = A + (k + 1 + i) * lda + (k + 1);
-        for (int j = tj; j < L; j += 16) {
-          const float2 uj = T->u[j];
+        float2* Ar = A22 + i * lda;
+        for (int j = tj; j <= i; j += 16) {
+          const float2 uj = U[j];
           const float2 wj = csub(T->p[j], cscale(uj, K));
-          Ar[j] = csub(csub(Ar[j], cmul_bc(ui, wj)), cmul_bc(wi, uj));
+          const float2 a = csub(csub(Ar[j], cmul_bc(ui, wj)), cmul_bc(wi, uj));
+          Ar[j] = a;
+          if (j == 0 && i >= 1) {
+            T->u[nxt][i - 1] = a;
+            nacc += cabs2(a);
+          }
         }
+      }
+      if (tj == 0) T->nrm[ti] = nacc;
+    } else {
+      if (warp == 0) {  // no reflection: column k+1 is unchanged
+        float s2 = 0.f;
+        for (int i = lane; i < L - 1; i += 32) {
+          const float2 x = A22[(1 + i) * lda];
+          s2 += cabs2(x);
+          T->u[nxt][i] = x;
+        }
+        s2 = warp_sum(s2);
+        if (lane == 0) T->nrm[0] = s2;
       }
     }
     __syncthreads();
@@ -142,47 +180,73 @@ __device__ __forceinline__ int sturm_count(const float* d, const float* e2, int 
   return c;
 }
 
-// Real form T' (D), Gershgorin interval, and the active index range (eigenvalues
-// n_below .. n_below + ra - 1 in ascending order).
+// Real form T' (D as a prefix product of unit phases), Gershgorin interval and the kept
+// index range (eigenvalues n_below .. n - 1 in ascending order); warp 0 only.
 template <int NPMAX>
 __device__ void tridiag_setup(TrdSmem<NPMAX>* T, int n, int mode, int rank, float lam, Misc* misc) {
-  if (threadIdx.x == 0) {
-    float2 dl = make_float2(1.f, 0.f);
-    float e2max = 0.f;
-    for (int k = 0; k < n; ++k) {
-      T->delta[k] = dl;
+  if ((threadIdx.x >> 5) == 0) {
+    const int lane = threadIdx.x & 31;
+    float2 ph[2];
+    float e2m = 0.f;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int k = 2 * lane + h;
+      ph[h] = make_float2(1.f, 0.f);
       if (k + 1 < n) {
         const float2 ek = T->e[k];
         const float a = sqrtf(cabs2(ek));
         T->ae[k] = a;
         T->e2[k] = a * a;
-        e2max = fmaxf(e2max, a * a);
-        if (a > 0.f) dl = cmul(dl, make_float2(ek.x / a, ek.y / a));
-      } else {
+        e2m = fmaxf(e2m, a * a);
+        if (a > 0.f) ph[h] = make_float2(ek.x / a, ek.y / a);
+      } else if (k < n) {
         T->ae[k] = 0.f;
         T->e2[k] = 0.f;
       }
     }
-    float gl = 3.0e38f, gu = -3.0e38f;
-    for (int k = 0; k < n; ++k) {
-      const float r = (k > 0 ? T->ae[k - 1] : 0.f) + (k + 1 < n ? T->ae[k] : 0.f);
-      gl = fminf(gl, T->d[k] - r);
-      gu = fmaxf(gu, T->d[k] + r);
+    // exclusive prefix product: delta_k = prod_{i<k} ph_i (complex products commute)
+    float2 pr = cmul(ph[0], ph[1]);
+    for (int o = 1; o < 32; o <<= 1) {
+      const float ox = __shfl_up_sync(0xffffffffu, pr.x, o), oy = __shfl_up_sync(0xffffffffu, pr.y, o);
+      if (lane >= o) pr = cmul(make_float2(ox, oy), pr);
     }
-    const float tn = fmaxf(fabsf(gl), fabsf(gu));
-    gl -= 4.f * 1.1920929e-7f * tn * n + 1e-30f;
-    gu += 4.f * 1.1920929e-7f * tn * n + 1e-30f;
-    misc->gl = gl;
-    misc->gu = gu;
-    misc->tnorm = tn;
-    misc->pivmin = 1.1754944e-38f * fmaxf(1.f, e2max);
-    int nb;
-    if (mode == LLR_PROX_HARD_RANK) nb = max(0, n - rank);
-    else if (!(lam > 0.f)) nb = 0;
-    else nb = sturm_count(T->d, T->e2, n, lam * lam, misc->pivmin);
-    misc->n_below = nb;
-    misc->ra = n - nb;
-    misc->fail = 0;
+    float ex = __shfl_up_sync(0xffffffffu, pr.x, 1), ey = __shfl_up_sync(0xffffffffu, pr.y, 1);
+    if (lane == 0) { ex = 1.f; ey = 0.f; }
+    const float2 excl = make_float2(ex, ey);
+    if (2 * lane < n) T->delta[2 * lane] = excl;
+    if (2 * lane + 1 < n) T->delta[2 * lane + 1] = cmul(excl, ph[0]);
+    __syncwarp();
+    float gl = 3.0e38f, gu = -3.0e38f;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int k = 2 * lane + h;
+      if (k < n) {
+        const float r = (k > 0 ? T->ae[k - 1] : 0.f) + (k + 1 < n ? T->ae[k] : 0.f);
+        gl = fminf(gl, T->d[k] - r);
+        gu = fmaxf(gu, T->d[k] + r);
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      gl = fminf(gl, __shfl_xor_sync(0xffffffffu, gl, o));
+      gu = fmaxf(gu, __shfl_xor_sync(0xffffffffu, gu, o));
+      e2m = fmaxf(e2m, __shfl_xor_sync(0xffffffffu, e2m, o));
+    }
+    if (lane == 0) {
+      const float tn = fmaxf(fabsf(gl), fabsf(gu));
+      gl -= 4.f * 1.1920929e-7f * tn * n + 1e-30f;
+      gu += 4.f * 1.1920929e-7f * tn * n + 1e-30f;
+      misc->gl = gl;
+      misc->gu = gu;
+      misc->tnorm = tn;
+      misc->pivmin = 1.1754944e-38f * fmaxf(1.f, e2m);
+      int nb;
+      if (mode == LLR_PROX_HARD_RANK) nb = max(0, n - rank);
+      else if (!(lam > 0.f)) nb = 0;
+      else nb = sturm_count(T->d, T->e2, n, lam * lam, misc->pivmin);
+      misc->n_below = nb;
+      misc->ra = n - nb;
+      misc->fail = 0;
+    }
   }
   __syncthreads();
 }
@@ -220,13 +284,14 @@ __device__ void tridiag_eigenvalues(TrdSmem<NPMAX>* T, int n, int j0, int count,
   __syncthreads();
 }
 
-// Inverse iteration (one thread per active eigenvalue) on T' - lambda I with partial
-// pivoting; three solves from a deterministic start vector.
+// Eigenvectors of T' (one thread per kept eigenvalue) from the twisted factorisation
+// T' - lam I = L+ D+ L+^T = U- D- U-^T; the twist r minimises |gamma_r|, z_r = 1 and the
+// two bidiagonal recurrences fill the rest.  `work` holds 2 * NPMAX * kRaMax floats.
 template <int NPMAX>
-__device__ void tridiag_vectors(TrdSmem<NPMAX>* T, int n, int ra, Misc* misc) {
+__device__ void tridiag_vectors(TrdSmem<NPMAX>* T, int n, int ra, Misc* misc, float* work) {
   const float eps = 1.1920929e-7f;
   const float tiny = eps * fmaxf(misc->tnorm, 1e-30f);
-  if (threadIdx.x == 0) {  // separate (near-)equal eigenvalues (LAPACK stein convention)
+  if (threadIdx.x == 0) {  // separate (near-)equal eigenvalues
     const float sep = 10.f * eps * fmaxf(misc->tnorm, 1e-30f);
     for (int a = 1; a < ra; ++a)
       if (T->lam[a] - T->lam[a - 1] < sep) T->lam[a] = T->lam[a - 1] + sep;
@@ -234,63 +299,42 @@ __device__ void tridiag_vectors(TrdSmem<NPMAX>* T, int n, int ra, Misc* misc) {
   __syncthreads();
   for (int a = threadIdx.x; a < ra; a += blockDim.x) {
     const float lam = T->lam[a];
-    float dd[NPMAX], du[NPMAX], du2[NPMAX], dl[NPMAX], b[NPMAX];
-    unsigned long long piv = 0ull;
-    for (int i = 0; i < n; ++i) {
-      dd[i] = T->d[i] - lam;
-      du[i] = (i + 1 < n) ? T->ae[i] : 0.f;
-      dl[i] = du[i];
-      du2[i] = 0.f;
-    }
+    float* Lp = work + a;                    // stride kRaMax
+    float* Dp = work + NPMAX * kRaMax + a;   // D+ then reused for U-
+    float dp = T->d[0] - lam;
     for (int i = 0; i + 1 < n; ++i) {
-      if (fabsf(dd[i]) >= fabsf(dl[i])) {
-        if (fabsf(dd[i]) < tiny) dd[i] = copysignf(tiny, dd[i] == 0.f ? 1.f : dd[i]);
-        const float f = dl[i] * __frcp_rn(dd[i]);
-        dl[i] = f;
-        dd[i + 1] -= f * du[i];
-      } else {
-        const float f = dd[i] * __frcp_rn(dl[i]);
-        dd[i] = dl[i];
-        dl[i] = f;
-        const float tmp = du[i];
-        du[i] = dd[i + 1];
-        dd[i + 1] = tmp - f * dd[i + 1];
-        if (i + 2 < n) {
-          du2[i] = du[i + 1];
-          du[i + 1] = -f * du[i + 1];
-        }
-        piv |= (1ull << i);
-      }
+      if (fabsf(dp) < tiny) dp = copysignf(tiny, dp);
+      Dp[i * kRaMax] = dp;
+      const float l = T->ae[i] * __frcp_rn(dp);
+      Lp[i * kRaMax] = l;
+      dp = T->d[i + 1] - lam - l * T->ae[i];
     }
-    if (fabsf(dd[n - 1]) < tiny) dd[n - 1] = copysignf(tiny, dd[n - 1] == 0.f ? 1.f : dd[n - 1]);
-    for (int i = 0; i < n; ++i) dd[i] = __frcp_rn(dd[i]);  // keep reciprocals of the pivots
-    uint64_t h = llr_splitmix64(0x1234567ull + (uint64_t)a);
-    for (int i = 0; i < n; ++i) {
-      h = llr_splitmix64(h);
-      b[i] = (float)((h >> 40) & 0xffffff) * (1.f / 16777216.f) - 0.5f;
+    if (fabsf(dp) < tiny) dp = copysignf(tiny, dp);
+    float dm = T->d[n - 1] - lam;
+    float best = fabsf(dp);  // gamma_{n-1} = D+_{n-1}
+    int r = n - 1;
+    for (int i = n - 2; i >= 0; --i) {
+      if (fabsf(dm) < tiny) dm = copysignf(tiny, dm);
+      const float um = T->ae[i] * __frcp_rn(dm);
+      const float dpi = Dp[i * kRaMax];
+      Dp[i * kRaMax] = um;                   // U-_i overwrites D+_i (no longer needed)
+      dm = T->d[i] - lam - um * T->ae[i];
+      const float gamma = dpi + dm - (T->d[i] - lam);
+      if (fabsf(gamma) < best) { best = fabsf(gamma); r = i; }
     }
-    for (int it = 0; it < 3; ++it) {
-      for (int i = 0; i + 1 < n; ++i) {
-        if (piv & (1ull << i)) {
-          const float t = b[i];
-          b[i] = b[i + 1];
-          b[i + 1] = t - dl[i] * b[i];
-        } else {
-          b[i + 1] -= dl[i] * b[i];
-        }
-      }
-      b[n - 1] *= dd[n - 1];
-      if (n >= 2) b[n - 2] = (b[n - 2] - du[n - 2] * b[n - 1]) * dd[n - 2];
-      for (int i = n - 3; i >= 0; --i) b[i] = (b[i] - du[i] * b[i + 1] - du2[i] * b[i + 2]) * dd[i];
-      float mx = 0.f;
-      for (int i = 0; i < n; ++i) mx = fmaxf(mx, fabsf(b[i]));
-      const float sc = mx > 0.f ? 1.f / mx : 1.f;
-      for (int i = 0; i < n; ++i) b[i] *= sc;
-    }
-    for (int i = 0; i < n; ++i) T->Y[a * NPMAX + i] = b[i];
+    float* y = T->Y + a * NPMAX;
+    float z = 1.f;
+    y[r] = 1.f;
+    for (int i = r - 1; i >= 0; --i) { z = -Lp[i * kRaMax] * z; y[i] = z; }
+    z = 1.f;
+    for (int i = r; i + 1 < n; ++i) { z = -Dp[i * kRaMax] * z; y[i + 1] = z; }
+    float mx = 0.f;
+    for (int i = 0; i < n; ++i) mx = fmaxf(mx, fabsf(y[i]));
+    const float sc = (mx > 0.f && mx < 3.0e38f) ? 1.f / mx : 0.f;
+    for (int i = 0; i < n; ++i) y[i] *= sc;
   }
   __syncthreads();
-  // modified Gram-Schmidt over the active vectors + residual check (warp 0)
+  // modified Gram-Schmidt over the kept vectors + residual check (warp 0)
   if ((threadIdx.x >> 5) == 0) {
     const int lane = threadIdx.x & 31;
     const float tol = 2e-5f * fmaxf(misc->tnorm, 1e-30f);
@@ -299,34 +343,32 @@ __device__ void tridiag_vectors(TrdSmem<NPMAX>* T, int n, int ra, Misc* misc) {
       float* y = T->Y + a * NPMAX;
       float y0 = lane < n ? y[lane] : 0.f, y1 = lane + 32 < n ? y[lane + 32] : 0.f;
       for (int c = 0; c < a; ++c) {
-        const float* z = T->Y + c * NPMAX;
-        const float z0 = lane < n ? z[lane] : 0.f, z1 = lane + 32 < n ? z[lane + 32] : 0.f;
-        float dp = y0 * z0 + y1 * z1;
-        for (int o = 16; o > 0; o >>= 1) dp += __shfl_xor_sync(0xffffffffu, dp, o);
-        y0 -= dp * z0;
-        y1 -= dp * z1;
+        const float* zc = T->Y + c * NPMAX;
+        const float z0 = lane < n ? zc[lane] : 0.f, z1 = lane + 32 < n ? zc[lane + 32] : 0.f;
+        const float dpr = warp_sum(y0 * z0 + y1 * z1);
+        y0 -= dpr * z0;
+        y1 -= dpr * z1;
       }
-      float nn = y0 * y0 + y1 * y1;
-      for (int o = 16; o > 0; o >>= 1) nn += __shfl_xor_sync(0xffffffffu, nn, o);
+      const float nn = warp_sum(y0 * y0 + y1 * y1);
       const float inv = nn > 0.f ? rsqrtf(nn) : 0.f;
       y0 *= inv;
       y1 *= inv;
       if (lane < n) y[lane] = y0;
       if (lane + 32 < n) y[lane + 32] = y1;
       __syncwarp();
-      // residual |T' y - lambda y|
       const float lam = T->lam[a];
       float r2 = 0.f;
+#pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int i = lane + 32 * h;
         if (i < n) {
-          float r = (T->d[i] - lam) * y[i];
-          if (i > 0) r += T->ae[i - 1] * y[i - 1];
-          if (i + 1 < n) r += T->ae[i] * y[i + 1];
-          r2 += r * r;
+          float rr = (T->d[i] - lam) * y[i];
+          if (i > 0) rr += T->ae[i - 1] * y[i - 1];
+          if (i + 1 < n) rr += T->ae[i] * y[i + 1];
+          r2 += rr * rr;
         }
       }
-      for (int o = 16; o > 0; o >>= 1) r2 += __shfl_xor_sync(0xffffffffu, r2, o);
+      r2 = warp_sum(r2);
       if (!(nn > 0.f) || !(sqrtf(r2) <= tol)) bad = 1;
       __syncwarp();
     }
@@ -349,25 +391,20 @@ __device__ void tridiag_backtransform(const float2* A, TrdSmem<NPMAX>* T, float2
     for (int k = n - 3; k >= 0; --k) {
       const float t = T->tau[k];
       if (t == 0.f) continue;
-      // u_k lives in column k of A below the diagonal (rows k+1 .. n-1), with u_k[0] at row k+1
-      // replaced by the value kept in column k during the reduction.
       const float2 u0 = (i0 > k && i0 < n) ? A[i0 * lda + k] : make_float2(0.f, 0.f);
       const float2 u1 = (i1 > k && i1 < n) ? A[i1 * lda + k] : make_float2(0.f, 0.f);
-      float2 s = cadd(cmulc(u0, v0), cmulc(u1, v1));
-      for (int o = 16; o > 0; o >>= 1) {
-        s.x += __shfl_xor_sync(0xffffffffu, s.x, o);
-        s.y += __shfl_xor_sync(0xffffffffu, s.y, o);
-      }
-      s = cscale(s, t);
-      v0 = csub(v0, cmul(u0, s));
-      v1 = csub(v1, cmul(u1, s));
+      float2 sv = cadd(cmulc(u0, v0), cmulc(u1, v1));
+      sv.x = warp_sum(sv.x);
+      sv.y = warp_sum(sv.y);
+      sv = cscale(sv, t);
+      v0 = csub(v0, cmul(u0, sv));
+      v1 = csub(v1, cmul(u1, sv));
     }
     if (i0 < n) V[i0 * kRaMax + a] = v0;
     if (i1 < n) V[i1 * kRaMax + a] = v1;
   }
   __syncthreads();
 }
-
 
 // ---------------------------------------------------------------------------------------
 // Per-block row tables: element (r, q) of the Casorati matrix lives at off[r] + q * qstride,
@@ -430,7 +467,8 @@ TrdLayout make_trd_layout(int m, int n) {
   L.off_C = off;
   const size_t chunk = sizeof(float2) * (size_t)n * L.ldch;
   const size_t scr = L.ksplit > 1 ? sizeof(float2) * (size_t)L.ksplit * L.np * L.np : 0;
-  off = align16(off + std::max(chunk, scr));
+  const size_t vec = sizeof(float) * 2 * NPMAX * kRaMax;   // twisted-factorisation work
+  off = align16(off + std::max(std::max(chunk, scr), vec));
   L.off_trd = off; off = align16(off + sizeof(TrdSmem<NPMAX>));
   L.off_V = off; off = align16(off + sizeof(float2) * NPMAX * kRaMax);
   L.off_g = off; off = align16(off + sizeof(float) * kRaMax);
@@ -441,16 +479,25 @@ TrdLayout make_trd_layout(int m, int n) {
 template <int RM>
 __device__ void apply_rows(const BlockSource& s, long long base, const RowTab* rows, const float2* rowph, int m, int n,
                            long long qstride, const float2* Va, const float* g, int ra) {
+  constexpr int KB = 8;   // loads in flight per thread
   for (int r = threadIdx.x; r < m; r += blockDim.x) {
     const RowTab rt = rows[r];
     float2 t[RM];
 #pragma unroll
     for (int a = 0; a < RM; ++a) t[a] = make_float2(0.f, 0.f);
-    for (int k = 0; k < n; ++k) {
-      const float2 c = load_elem(s, base, rt, rowph, r, k, qstride);
+    for (int k0 = 0; k0 < n; k0 += KB) {
+      float2 c[KB];
 #pragma unroll
-      for (int a = 0; a < RM; ++a)
-        if (a < ra) cfma(t[a], c, Va[k * kRaMax + a]);
+      for (int u = 0; u < KB; ++u)
+        c[u] = (k0 + u < n) ? load_elem(s, base, rt, rowph, r, k0 + u, qstride) : make_float2(0.f, 0.f);
+#pragma unroll
+      for (int u = 0; u < KB; ++u) {
+        if (k0 + u < n) {
+#pragma unroll
+          for (int a = 0; a < RM; ++a)
+            if (a < ra) cfma(t[a], c[u], Va[(k0 + u) * kRaMax + a]);
+        }
+      }
     }
 #pragma unroll
     for (int a = 0; a < RM; ++a)
@@ -519,15 +566,42 @@ __global__ void __launch_bounds__(kLlrThreads, 2) llr_prox_trd_kernel(BlockSourc
     for (int c0 = 0; c0 < m; c0 += L.rc) {
       const int rc = min(L.rc, m - c0);
       {
+        constexpr int GB = 8;   // loads in flight per thread
         const int tot = rc * n;
         int q = tid / rc, rr = tid - (tid / rc) * rc;
         const int sq = blockDim.x / rc, sr = blockDim.x - sq * rc;
-        for (int i = tid; i < tot; i += blockDim.x) {
-          const int r = c0 + rr;
-          Cch[q * L.ldch + rr] = load_elem(src, base, rows[r], rowph, r, q, qstride);
-          rr += sr;
-          q += sq;
-          if (rr >= rc) { rr -= rc; ++q; }
+        for (int i0 = tid; i0 < tot; i0 += GB * blockDim.x) {
+          float2 v[GB];
+          int dq[GB], dr[GB];
+#pragma unroll
+          for (int u = 0; u < GB; ++u) {
+            dq[u] = q;
+            dr[u] = rr;
+            if (i0 + u * (int)blockDim.x < tot) {
+              const RowTab rt = rows[c0 + rr];
+              v[u] = src.data[base + (long long)rt.off + (long long)q * qstride];
+            }
+            rr += sr;
+            q += sq;
+            if (rr >= rc) { rr -= rc; ++q; }
+          }
+#pragma unroll
+          for (int u = 0; u < GB; ++u) {
+            if (i0 + u * (int)blockDim.x < tot) {
+              const int r = c0 + dr[u];
+              float2 x = v[u];
+              if (src.kind == 1) {
+                float2 p;
+                if (src.ph_uniform) p = rowph[r];
+                else {
+                  const RowTab rt = rows[r];
+                  p = phase_at(src.ph, src.g, dq[u], rt.cx, rt.cyz & 0xffff, rt.cyz >> 16);
+                }
+                x = cscale(cmul_bc(x, p), src.load_scale);
+              }
+              Cch[dq[u] * L.ldch + dr[u]] = x;
+            }
+          }
         }
       }
       __syncthreads();
@@ -603,7 +677,7 @@ __global__ void __launch_bounds__(kLlrThreads, 2) llr_prox_trd_kernel(BlockSourc
     bool fallback = ra > kRaMax;
     if (!fallback) {
       tridiag_eigenvalues<NPMAX>(trd, n, nb, ra, misc);
-      tridiag_vectors<NPMAX>(trd, n, ra, misc);
+      tridiag_vectors<NPMAX>(trd, n, ra, misc, reinterpret_cast<float*>(Cch));
       fallback = misc->fail != 0;
     }
     if (fallback) {
