@@ -161,6 +161,18 @@ int llr_un_lift_data_set_dev(llr_cf32* d_vol, int32_t nq, const llr_cf32* d_mat,
 /* cu_low_rank_approx_batch (low_rank.rs:10-69) in place on (m, n, batch), n <= 64. */
 int llr_low_rank_batch_dev(int32_t m, int32_t n, int32_t rank, int32_t batch,
                            llr_cf32* d_mats, void* stream);
+/* Same operation as llr_low_rank_batch_dev, for callers that cannot let the library
+ * allocate device memory (a caller replaying its own CUDA graph under a fixed memory plan,
+ * a device whose memory belongs to another framework's pool, a loop that must not pay an
+ * allocator call per invocation).  No counterpart in the reference.  It allocates nothing:
+ * its scratch is a static 256 KiB device array per GPU (held until exit), so batch must be
+ * <= 65536 (LLR_ERR_INVALID otherwise).  The first call on a device looks up that array's
+ * device address; make that first call before any stream capture.  All calls on a GPU
+ * share the array and it keeps the last call's contents (the count word is cleared by every
+ * call), so calls that can run at the same time on one GPU, e.g. on two streams, race:
+ * serialise them. */
+int llr_low_rank_batch_dev_noalloc(int32_t m, int32_t n, int32_t rank, int32_t batch,
+                                   llr_cf32* d_mats, void* stream);
 /* Singular-value soft threshold of every (m, n) matrix, n <= 64. */
 int llr_soft_threshold_batch_dev(int32_t m, int32_t n, float lambda, int32_t batch,
                                  llr_cf32* d_mats, void* stream);

@@ -117,6 +117,7 @@ SIGNATURES = {
     "llr_lift_data_set_dev": (C.c_int, [P, I32, P, PI32, PI32, PI32, I64, I64, P]),
     "llr_un_lift_data_set_dev": (C.c_int, [P, I32, P, PI32, PI32, PI32, I64, I64, P]),
     "llr_low_rank_batch_dev": (C.c_int, [I32, I32, I32, I32, P, P]),
+    "llr_low_rank_batch_dev_noalloc": (C.c_int, [I32, I32, I32, I32, P, P]),
     "llr_soft_threshold_batch_dev": (C.c_int, [I32, I32, F32, I32, P, P]),
     "llr_subspace_low_rank_batch_dev": (C.c_int, [I32, I32, I32, I32, I32, F32, P, I32, P, P]),
     "rhsCdgmmBatched": (C.c_int, [C.c_int, C.c_int, C.c_int, P, P]),
