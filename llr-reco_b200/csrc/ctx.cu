@@ -190,6 +190,7 @@ static int prox_pass(llr_ctx* c, cudaStream_t s, const int* explicit_shift, bool
     op.eig_solver = c->cfg.eig_solver;
     op.fb_list = c->d_fb;
     op.fb_count = c->d_fb + std::max<long long>(1, c->nblocks);
+    op.gram = c->d_gram;
     LLR_TRY(launch_llr_prox(src, op, s));
   }
   if (block_stat || standalone) return LLR_OK;
@@ -287,6 +288,9 @@ int llr_ctx_create(const llr_config* cfg, llr_ctx** out) {
   if ((st = dalloc(&c->d_iter, 1))) return fail(st);
   if ((st = dalloc(&c->d_block_stat, (size_t)std::max<long long>(1, c->nblocks)))) return fail(st);
   if ((st = dalloc(&c->d_fb, (size_t)std::max<long long>(1, c->nblocks) + 1))) return fail(st);
+  if (cfg->subspace_rank == 0 &&
+      (st = dalloc(&c->d_gram, (size_t)std::max<long long>(1, c->nblocks) * ((size_t)c->g.nq * (c->g.nq + 1) / 2))))
+    return fail(st);
   e = cudaMemsetAsync(c->d_iter, 0, sizeof(long long), c->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(c->d_hist, 0, sizeof(double) * c->hist_cap, c->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(c->d_x, 0, sizeof(float2) * E, c->stream);
@@ -320,7 +324,7 @@ int llr_ctx_destroy(llr_ctx* c) {
   if (c->have_plan) cufftDestroy(c->plan_fwd);
   dfree(c->d_x); dfree(c->d_work); dfree(c->d_yhat); dfree(c->d_samp_pos); dfree(c->d_samp_off);
   dfree(c->d_ph_ksp); dfree(c->d_ph_img); dfree(c->d_S); dfree(c->d_partials); dfree(c->d_hist); dfree(c->d_iter);
-  dfree(c->d_block_stat); dfree(c->d_fb); dfree(c->d_wavelet_work); dfree(c->d_fft_work);
+  dfree(c->d_block_stat); dfree(c->d_fb); dfree(c->d_gram); dfree(c->d_wavelet_work); dfree(c->d_fft_work);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return LLR_OK;

@@ -356,12 +356,21 @@ static int batch_prox(int m, int n, int mode, int rank, float lam, int batch, ll
   op.m = m; op.n = n; op.mode = mode; op.rank = rank; op.lambda = lam; op.block_stat = nullptr;
   op.eig_solver = g_batch_eig_solver;
   int* fb = nullptr;
+  float2* gram = nullptr;
   LLR_CUDA_TRY(cudaMallocAsync((void**)&fb, sizeof(int) * ((size_t)batch + 1), s));
+  cudaError_t e = cudaMallocAsync((void**)&gram, sizeof(float2) * (size_t)batch * ((size_t)n * (n + 1) / 2), s);
+  if (e != cudaSuccess) {
+    cudaFreeAsync(fb, s);
+    return cuda_error(e, "cudaMallocAsync", __FILE__, __LINE__);
+  }
   op.fb_list = fb;
   op.fb_count = fb + batch;
+  op.gram = gram;
   int st = launch_llr_prox(src, op, s);
-  cudaError_t e = cudaFreeAsync(fb, s);
+  e = cudaFreeAsync(fb, s);
+  cudaError_t e2 = cudaFreeAsync(gram, s);
   if (st == LLR_OK && e != cudaSuccess) st = cuda_error(e, "cudaFreeAsync", __FILE__, __LINE__);
+  if (st == LLR_OK && e2 != cudaSuccess) st = cuda_error(e2, "cudaFreeAsync", __FILE__, __LINE__);
   return st;
 }
 

@@ -42,6 +42,7 @@ struct ProxOp {
   int eig_solver;      // 0: tridiagonal + bisection + inverse iteration; 1: Jacobi
   int* fb_list;        // blocks handed to the Jacobi kernel (capacity nblocks)
   int* fb_count;
+  float2* gram;        // optional scratch, nblocks * n(n+1)/2: selects the split Gram/eigen path
 };
 
 int launch_llr_prox(const BlockSource& src, const ProxOp& op, cudaStream_t stream);
@@ -120,6 +121,7 @@ struct llr_ctx {
   long long h_iter;         // host mirror (valid after sync)
   float* d_block_stat;
   int* d_fb;                // Jacobi fallback block list (nblocks) + count
+  float2* d_gram;           // per-block packed Gram matrices (split prox path)
   int ph_uniform;           // all volumes share the image-domain phase tables
   float2* d_wavelet_work;
   size_t wavelet_work_elems;

@@ -41,6 +41,15 @@ struct TrdSmem {
   float Y[NPMAX * kRaMax];  // eigenvectors of T', column a at Y[a * NPMAX]
 };
 
+// Element (i, j), j <= i, of the Gram matrix in shared memory: full row-major storage with
+// leading dimension NPMAX + 1, or packed lower triangle i(i+1)/2 + j.
+template <int NPMAX, bool PACKED>
+struct AIdx {
+  __device__ __forceinline__ static int at(int i, int j) {
+    return PACKED ? (i * (i + 1)) / 2 + j : i * (NPMAX + 1) + j;
+  }
+};
+
 __device__ __forceinline__ float warp_sum(float v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
@@ -57,17 +66,18 @@ __device__ __forceinline__ float warp_sum(float v) {
 // sweeps * 8 n^3 for Jacobi; blocks whose eigenvectors fail the residual check go to the
 // Jacobi kernel.
 // =======================================================================================
-template <int NPMAX>
+template <int NPMAX, bool PACKED>
 __device__ void hermitian_tridiag(float2* A, int n, TrdSmem<NPMAX>* T, float* red) {
-  constexpr int lda = NPMAX + 1;
+  typedef AIdx<NPMAX, PACKED> I;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nwarps = blockDim.x >> 5;
-  const int tj = tid & 15, ti = tid >> 4;
+  const int tj = tid & 15, ti = tid >> 4, TI = blockDim.x >> 4;   // 16-wide update grid
+  const int tpr = blockDim.x >> 6;                                  // matvec threads per row
   if (n >= 3) {  // vector and norm of column 0; later columns come from the previous update
     if (warp == 0) {
       float s2 = 0.f;
       for (int i = lane; i < n - 1; i += 32) {
-        const float2 x = A[(1 + i) * lda];
+        const float2 x = A[I::at(1 + i, 0)];
         s2 += cabs2(x);
         T->u[0][i] = x;
       }
@@ -80,10 +90,11 @@ __device__ void hermitian_tridiag(float2* A, int n, TrdSmem<NPMAX>* T, float* re
     const int L = n - k - 1;
     const int cur = k & 1, nxt = cur ^ 1;
     float2* U = T->u[cur];
+    const int o = k + 1;   // A22 starts at (o, o)
     if (tid == 0) {
       float s2 = 0.f;
       for (int i = 0; i < 16; ++i) { s2 += T->nrm[i]; T->nrm[i] = 0.f; }
-      const float2 x0 = A[(k + 1) * lda + k];
+      const float2 x0 = A[I::at(o, k)];
       const float xn = sqrtf(s2);
       const float aa = sqrtf(cabs2(x0));
       const float phx = aa > 0.f ? x0.x / aa : 1.f, phy = aa > 0.f ? x0.y / aa : 0.f;
@@ -92,26 +103,25 @@ __device__ void hermitian_tridiag(float2* A, int n, TrdSmem<NPMAX>* T, float* re
       const float t = (xn > 0.f && un2 > 0.f) ? 2.f / un2 : 0.f;
       T->tau[k] = t;
       T->e[k] = make_float2(-phx * xn, -phy * xn);
-      A[(k + 1) * lda + k] = u0;  // column k keeps u_k for the back-transformation
+      A[I::at(o, k)] = u0;  // column k keeps u_k for the back-transformation
       U[0] = u0;
     }
     __syncthreads();
     const float t = T->tau[k];
-    float2* A22 = A + (k + 1) * lda + (k + 1);
     if (t != 0.f) {
       // p = t * A22 u from the lower triangle (A22[i][j] = conj(A22[j][i]) for j > i)
-      const int row = tid >> 2, part = tid & 3;
+      const int row = tid / tpr, part = tid - row * tpr;
       float2 acc = make_float2(0.f, 0.f);
       if (row < L) {
-        for (int j = part; j < L; j += 4) {
-          const float2 a = (j <= row) ? A22[row * lda + j] : cconj(A22[j * lda + row]);
+        for (int j = part; j < L; j += tpr) {
+          const float2 a = (j <= row) ? A[I::at(o + row, o + j)] : cconj(A[I::at(o + j, o + row)]);
           cfma(acc, a, U[j]);
         }
       }
-      acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 1);
-      acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 1);
-      acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 2);
-      acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 2);
+      for (int sft = 1; sft < tpr; sft <<= 1) {
+        acc.x += __shfl_xor_sync(0xffffffffu, acc.x, sft);
+        acc.y += __shfl_xor_sync(0xffffffffu, acc.y, sft);
+      }
       float dp = 0.f;
       if (row < L && part == 0) {
         const float2 pv = cscale(acc, t);
@@ -128,15 +138,15 @@ __device__ void hermitian_tridiag(float2* A, int n, TrdSmem<NPMAX>* T, float* re
       // lower-triangle update A22 -= u w^H + w u^H,  w = p - K u; the threads of column 0
       // also hand the next step its x vector and the partial norms.
       float nacc = 0.f;
-      for (int i = ti; i < L; i += 16) {
+      for (int i = ti; i < L; i += TI) {
         const float2 ui = U[i];
         const float2 wi = csub(T->p[i], cscale(ui, K));
-        float2* Ar = A22 + i * lda;
+        const int rb = I::at(o + i, o);
         for (int j = tj; j <= i; j += 16) {
           const float2 uj = U[j];
           const float2 wj = csub(T->p[j], cscale(uj, K));
-          const float2 a = csub(csub(Ar[j], cmul_bc(ui, wj)), cmul_bc(wi, uj));
-          Ar[j] = a;
+          const float2 a = csub(csub(A[rb + j], cmul_bc(ui, wj)), cmul_bc(wi, uj));
+          A[rb + j] = a;
           if (j == 0 && i >= 1) {
             T->u[nxt][i - 1] = a;
             nacc += cabs2(a);
@@ -148,7 +158,7 @@ __device__ void hermitian_tridiag(float2* A, int n, TrdSmem<NPMAX>* T, float* re
       if (warp == 0) {  // no reflection: column k+1 is unchanged
         float s2 = 0.f;
         for (int i = lane; i < L - 1; i += 32) {
-          const float2 x = A22[(1 + i) * lda];
+          const float2 x = A[I::at(o + 1 + i, o)];
           s2 += cabs2(x);
           T->u[nxt][i] = x;
         }
@@ -158,9 +168,9 @@ __device__ void hermitian_tridiag(float2* A, int n, TrdSmem<NPMAX>* T, float* re
     }
     __syncthreads();
   }
-  if (tid < n) T->d[tid] = A[tid * lda + tid].x;
+  if (tid < n) T->d[tid] = A[I::at(tid, tid)].x;
   if (tid == 0) {
-    if (n >= 2) T->e[n - 2] = A[(n - 1) * lda + n - 2];
+    if (n >= 2) T->e[n - 2] = A[I::at(n - 1, n - 2)];
     for (int k = n - 2; k < n; ++k)
       if (k >= 0) T->tau[k] = 0.f;
   }
@@ -378,9 +388,9 @@ __device__ void tridiag_vectors(TrdSmem<NPMAX>* T, int n, int ra, Misc* misc, fl
 }
 
 // Va[i * kRaMax + a] = (Q D y_a)_i (complex), one warp per vector.
-template <int NPMAX>
+template <int NPMAX, bool PACKED>
 __device__ void tridiag_backtransform(const float2* A, TrdSmem<NPMAX>* T, float2* V, int n, int ra) {
-  constexpr int lda = NPMAX + 1;
+  typedef AIdx<NPMAX, PACKED> I;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int a = warp; a < ra; a += nw) {
     const float* y = T->Y + a * NPMAX;
@@ -391,8 +401,8 @@ __device__ void tridiag_backtransform(const float2* A, TrdSmem<NPMAX>* T, float2
     for (int k = n - 3; k >= 0; --k) {
       const float t = T->tau[k];
       if (t == 0.f) continue;
-      const float2 u0 = (i0 > k && i0 < n) ? A[i0 * lda + k] : make_float2(0.f, 0.f);
-      const float2 u1 = (i1 > k && i1 < n) ? A[i1 * lda + k] : make_float2(0.f, 0.f);
+      const float2 u0 = (i0 > k && i0 < n) ? A[I::at(i0, k)] : make_float2(0.f, 0.f);
+      const float2 u1 = (i1 > k && i1 < n) ? A[I::at(i1, k)] : make_float2(0.f, 0.f);
       float2 sv = cadd(cmulc(u0, v0), cmulc(u1, v1));
       sv.x = warp_sum(sv.x);
       sv.y = warp_sum(sv.y);
@@ -512,27 +522,13 @@ __device__ void apply_rows(const BlockSource& s, long long base, const RowTab* r
   }
 }
 
-template <int NPMAX, int TG>
-__global__ void __launch_bounds__(kLlrThreads, 2) llr_prox_trd_kernel(BlockSource src, ProxOp op, TrdLayout L) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  Misc* misc = reinterpret_cast<Misc*>(smem);
-  RowTab* rows = reinterpret_cast<RowTab*>(smem + L.off_row);
-  float2* rowph = reinterpret_cast<float2*>(smem + L.off_rowph);
-  float2* A = reinterpret_cast<float2*>(smem + L.off_A);
-  float2* Cch = reinterpret_cast<float2*>(smem + L.off_C);
-  TrdSmem<NPMAX>* trd = reinterpret_cast<TrdSmem<NPMAX>*>(smem + L.off_trd);
-  float2* Va = reinterpret_cast<float2*>(smem + L.off_V);
-  float* g = reinterpret_cast<float*>(smem + L.off_g);
-  constexpr int lda = NPMAX + 1;
-  const int m = op.m, n = op.n, tid = threadIdx.x;
-  const long long qstride = src.kind == 1 ? src.g.V : (long long)m;
-
-  if (tid == 0) block_shift(src, misc->shift);
-  __syncthreads();
-  const int sh[3] = {misc->shift[0], misc->shift[1], misc->shift[2]};
-
-  for (long long blk = blockIdx.x; blk < src.nblocks; blk += gridDim.x) {
-    const long long base = src.kind == 1 ? 0 : blk * (long long)m * n;
+// Row tables of block `blk`, then its Gram matrix over staged row chunks (tile accumulators
+// in registers); every lower-or-upper element (i, j) < n is handed to sink(i, j, value).
+template <int NPMAX, int TG, class Sink>
+__device__ void gram_block(const BlockSource& src, const TrdLayout& L, int m, int n, long long blk,
+                           long long base, long long qstride, const int* sh, RowTab* rows, float2* rowph,
+                           float2* Cch, Sink sink) {
+  const int tid = threadIdx.x;
     // row tables
     for (int r = tid; r < m; r += blockDim.x) {
       RowTab rt;
@@ -630,7 +626,7 @@ __global__ void __launch_bounds__(kLlrThreads, 2) llr_prox_trd_kernel(BlockSourc
 #pragma unroll
           for (int b = 0; b < TG; ++b) {
             const int cI = ti + nt * a, cJ = tj + nt * b;
-            if (cI < n && cJ < n) A[cI * lda + cJ] = acc[a][b];
+            if (cI < n && cJ < n) sink(cI, cJ, acc[a][b]);
           }
       }
     } else {
@@ -647,12 +643,37 @@ __global__ void __launch_bounds__(kLlrThreads, 2) llr_prox_trd_kernel(BlockSourc
         const int i = idx / n, j = idx - i * n;
         float2 sacc = make_float2(0.f, 0.f);
         for (int k = 0; k < L.ksplit; ++k) sacc = cadd(sacc, P[(size_t)k * L.np * L.np + i * L.np + j]);
-        A[i * lda + j] = sacc;
+        sink(i, j, sacc);
       }
     }
     __syncthreads();
+}
 
-    hermitian_tridiag<NPMAX>(A, n, trd, misc->red);
+template <int NPMAX, int TG>
+__global__ void __launch_bounds__(kLlrThreads, 2) llr_prox_trd_kernel(BlockSource src, ProxOp op, TrdLayout L) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  Misc* misc = reinterpret_cast<Misc*>(smem);
+  RowTab* rows = reinterpret_cast<RowTab*>(smem + L.off_row);
+  float2* rowph = reinterpret_cast<float2*>(smem + L.off_rowph);
+  float2* A = reinterpret_cast<float2*>(smem + L.off_A);
+  float2* Cch = reinterpret_cast<float2*>(smem + L.off_C);
+  TrdSmem<NPMAX>* trd = reinterpret_cast<TrdSmem<NPMAX>*>(smem + L.off_trd);
+  float2* Va = reinterpret_cast<float2*>(smem + L.off_V);
+  float* g = reinterpret_cast<float*>(smem + L.off_g);
+  constexpr int lda = NPMAX + 1;
+  const int m = op.m, n = op.n, tid = threadIdx.x;
+  const long long qstride = src.kind == 1 ? src.g.V : (long long)m;
+
+  if (tid == 0) block_shift(src, misc->shift);
+  __syncthreads();
+  const int sh[3] = {misc->shift[0], misc->shift[1], misc->shift[2]};
+
+  for (long long blk = blockIdx.x; blk < src.nblocks; blk += gridDim.x) {
+    const long long base = src.kind == 1 ? 0 : blk * (long long)m * n;
+    gram_block<NPMAX, TG>(src, L, m, n, blk, base, qstride, sh, rows, rowph, Cch,
+                          [&](int i, int j, float2 v) { A[i * lda + j] = v; });
+
+    hermitian_tridiag<NPMAX, false>(A, n, trd, misc->red);
     if (op.block_stat) {
       tridiag_setup<NPMAX>(trd, n, LLR_PROX_HARD_RANK, 1, 0.f, misc);
       tridiag_eigenvalues<NPMAX>(trd, n, n - 1, 1, misc);
@@ -688,7 +709,7 @@ __global__ void __launch_bounds__(kLlrThreads, 2) llr_prox_trd_kernel(BlockSourc
       __syncthreads();
       continue;
     }
-    tridiag_backtransform<NPMAX>(A, trd, Va, n, ra);
+    tridiag_backtransform<NPMAX, false>(A, trd, Va, n, ra);
     if (tid < ra) {
       float gv = 1.f;
       if (op.mode != LLR_PROX_HARD_RANK) {
@@ -724,6 +745,178 @@ int launch_trd_instance(const BlockSource& src, const ProxOp& op, cudaStream_t s
   return LLR_OK;
 }
 
+// =======================================================================================
+// Split path.  llr_gram_kernel writes every block's Gram matrix (packed lower triangle,
+// n(n+1)/2 complex) to a scratch buffer; llr_eig_apply_kernel (128 threads, several CTAs per
+// SM so that several blocks' serial eigen phases overlap) reads it back into shared memory,
+// runs the tridiagonal eigen path and applies C' = (C V_a) g V_a^H from global to global.
+// =======================================================================================
+template <int NPMAX, int TG>
+__global__ void __launch_bounds__(kLlrThreads, 2) llr_gram_kernel(BlockSource src, ProxOp op, TrdLayout L) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  Misc* misc = reinterpret_cast<Misc*>(smem);
+  RowTab* rows = reinterpret_cast<RowTab*>(smem + L.off_row);
+  float2* rowph = reinterpret_cast<float2*>(smem + L.off_rowph);
+  float2* Cch = reinterpret_cast<float2*>(smem + L.off_C);
+  const int m = op.m, n = op.n;
+  const long long qstride = src.kind == 1 ? src.g.V : (long long)m;
+  const long long P = (long long)n * (n + 1) / 2;
+  if (threadIdx.x == 0) block_shift(src, misc->shift);
+  __syncthreads();
+  const int sh[3] = {misc->shift[0], misc->shift[1], misc->shift[2]};
+  for (long long blk = blockIdx.x; blk < src.nblocks; blk += gridDim.x) {
+    const long long base = src.kind == 1 ? 0 : blk * (long long)m * n;
+    float2* G = op.gram + blk * P;
+    gram_block<NPMAX, TG>(src, L, m, n, blk, base, qstride, sh, rows, rowph, Cch, [&](int i, int j, float2 v) {
+      if (j <= i) G[(i * (i + 1)) / 2 + j] = v;
+    });
+  }
+}
+
+constexpr int kEigThreads = 128;
+
+struct EigLayout {
+  size_t off_row, off_rowph, off_A, off_trd, off_V, off_g, off_work, total;
+};
+
+template <int NPMAX>
+EigLayout make_eig_layout(int m) {
+  EigLayout L;
+  size_t off = 256;
+  L.off_row = off; off = align16(off + sizeof(RowTab) * (size_t)m);
+  L.off_rowph = off; off = align16(off + sizeof(float2) * (size_t)m);
+  L.off_A = off; off = align16(off + sizeof(float2) * (size_t)NPMAX * (NPMAX + 1) / 2);
+  L.off_trd = off; off = align16(off + sizeof(TrdSmem<NPMAX>));
+  L.off_V = off; off = align16(off + sizeof(float2) * NPMAX * kRaMax);
+  L.off_g = off; off = align16(off + sizeof(float) * kRaMax);
+  L.off_work = off; off = align16(off + sizeof(float) * 2 * NPMAX * kRaMax);
+  L.total = off;
+  return L;
+}
+
+template <int NPMAX>
+__global__ void __launch_bounds__(kEigThreads, 4) llr_eig_apply_kernel(BlockSource src, ProxOp op, EigLayout L) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  Misc* misc = reinterpret_cast<Misc*>(smem);
+  RowTab* rows = reinterpret_cast<RowTab*>(smem + L.off_row);
+  float2* rowph = reinterpret_cast<float2*>(smem + L.off_rowph);
+  float2* A = reinterpret_cast<float2*>(smem + L.off_A);
+  TrdSmem<NPMAX>* trd = reinterpret_cast<TrdSmem<NPMAX>*>(smem + L.off_trd);
+  float2* Va = reinterpret_cast<float2*>(smem + L.off_V);
+  float* g = reinterpret_cast<float*>(smem + L.off_g);
+  float* work = reinterpret_cast<float*>(smem + L.off_work);
+  const int m = op.m, n = op.n, tid = threadIdx.x;
+  const long long qstride = src.kind == 1 ? src.g.V : (long long)m;
+  const int P = n * (n + 1) / 2;
+  if (tid == 0) block_shift(src, misc->shift);
+  __syncthreads();
+  const int sh[3] = {misc->shift[0], misc->shift[1], misc->shift[2]};
+
+  for (long long blk = blockIdx.x; blk < src.nblocks; blk += gridDim.x) {
+    const long long base = src.kind == 1 ? 0 : blk * (long long)m * n;
+    const float2* G = op.gram + blk * (long long)P;
+    for (int i = tid; i < P; i += blockDim.x) A[i] = G[i];
+    __syncthreads();
+    hermitian_tridiag<NPMAX, true>(A, n, trd, misc->red);
+    if (op.block_stat) {
+      tridiag_setup<NPMAX>(trd, n, LLR_PROX_HARD_RANK, 1, 0.f, misc);
+      tridiag_eigenvalues<NPMAX>(trd, n, n - 1, 1, misc);
+      if (tid == 0) op.block_stat[blk] = trd->lam[0];
+      __syncthreads();
+      continue;
+    }
+    tridiag_setup<NPMAX>(trd, n, op.mode, op.rank, op.lambda, misc);
+    const int ra = misc->ra, nb = misc->n_below;
+    if (ra == n && op.mode == LLR_PROX_HARD_RANK) {
+      __syncthreads();
+      continue;  // rank >= n: identity, nothing to write
+    }
+    // row tables (only the apply needs them here)
+    for (int r = tid; r < m; r += blockDim.x) {
+      RowTab rt;
+      if (src.kind == 1) {
+        int ix, iy, iz;
+        block_row_coord(src, blk, sh, r, ix, iy, iz);
+        rt.off = (int)planar_index(src.g, ix, iy, iz, 0);
+        rt.cx = ix;
+        rt.cyz = iy | (iz << 16);
+        if (src.ph_uniform) rowph[r] = phase_at(src.ph, src.g, 0, ix, iy, iz);
+      } else {
+        rt.off = r;
+        rt.cx = 0;
+        rt.cyz = 0;
+      }
+      rt.pad = 0;
+      rows[r] = rt;
+    }
+    __syncthreads();
+    if (ra == 0) {
+      for (int idx = tid; idx < m * n; idx += blockDim.x) {
+        const int q = idx / m, r = idx - q * m;
+        store_elem(src, base, rows[r], rowph, r, q, qstride, make_float2(0.f, 0.f));
+      }
+      __syncthreads();
+      continue;
+    }
+    bool fallback = ra > kRaMax;
+    if (!fallback) {
+      tridiag_eigenvalues<NPMAX>(trd, n, nb, ra, misc);
+      tridiag_vectors<NPMAX>(trd, n, ra, misc, work);
+      fallback = misc->fail != 0;
+    }
+    if (fallback) {
+      if (tid == 0 && op.fb_list) {
+        const int pos = atomicAdd(op.fb_count, 1);
+        op.fb_list[pos] = (int)blk;
+      }
+      __syncthreads();
+      continue;
+    }
+    tridiag_backtransform<NPMAX, true>(A, trd, Va, n, ra);
+    if (tid < ra) {
+      float gv = 1.f;
+      if (op.mode != LLR_PROX_HARD_RANK) {
+        const float sv = sqrtf(fmaxf(trd->lam[tid], 0.f));
+        gv = (sv > op.lambda) ? (1.f - op.lambda / sv) : 0.f;
+      }
+      g[tid] = gv;
+    }
+    __syncthreads();
+    if (ra <= 4) apply_rows<4>(src, base, rows, rowph, m, n, qstride, Va, g, ra);
+    else if (ra <= 8) apply_rows<8>(src, base, rows, rowph, m, n, qstride, Va, g, ra);
+    else apply_rows<kRaMax>(src, base, rows, rowph, m, n, qstride, Va, g, ra);
+    __syncthreads();
+  }
+}
+
+template <int NPMAX, int TG>
+int launch_split_instance(const BlockSource& src, const ProxOp& op, cudaStream_t stream) {
+  int dev = 0, nsm = 0, occ = 0;
+  LLR_CUDA_TRY(cudaGetDevice(&dev));
+  LLR_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  {
+    TrdLayout L = make_trd_layout<NPMAX, TG>(op.m, op.n);
+    auto kern = llr_gram_kernel<NPMAX, TG>;
+    LLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total));
+    LLR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kLlrThreads, L.total));
+    if (occ < 1) return set_error(LLR_ERR_UNSUPPORTED, "Gram kernel cannot be resident (smem %zu B)", L.total);
+    const long long grid = std::min<long long>(src.nblocks, (long long)nsm * occ);
+    kern<<<(unsigned)grid, kLlrThreads, L.total, stream>>>(src, op, L);
+    LLR_CUDA_TRY(cudaGetLastError());
+  }
+  {
+    EigLayout L = make_eig_layout<NPMAX>(op.m);
+    auto kern = llr_eig_apply_kernel<NPMAX>;
+    LLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total));
+    LLR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kEigThreads, L.total));
+    if (occ < 1) return set_error(LLR_ERR_UNSUPPORTED, "eigen kernel cannot be resident (smem %zu B)", L.total);
+    const long long grid = std::min<long long>(src.nblocks, (long long)nsm * occ);
+    kern<<<(unsigned)grid, kEigThreads, L.total, stream>>>(src, op, L);
+    LLR_CUDA_TRY(cudaGetLastError());
+  }
+  return LLR_OK;
+}
+
 }  // namespace
 
 bool llr_prox_supported(int m, int n) {
@@ -745,10 +938,16 @@ int launch_llr_prox(const BlockSource& src, const ProxOp& op, cudaStream_t strea
     return set_error(LLR_ERR_INVALID, "tridiagonal prox needs a fallback block list");
   if (op.fb_count) LLR_CUDA_TRY(cudaMemsetAsync(op.fb_count, 0, sizeof(int), stream));
   int st;
-  if (op.n <= 16) st = launch_trd_instance<16, 2>(src, op, stream);
-  else if (op.n <= 32) st = launch_trd_instance<32, 2>(src, op, stream);
-  else if (op.n <= 64) st = launch_trd_instance<64, 4>(src, op, stream);
-  else return set_error(LLR_ERR_UNSUPPORTED, "Casorati column count %d > 64 is not supported", op.n);
+  if (op.n > 64) return set_error(LLR_ERR_UNSUPPORTED, "Casorati column count %d > 64 is not supported", op.n);
+  if (op.gram) {  // split path: Gram kernel + eigen/apply kernel through the scratch buffer
+    if (op.n <= 16) st = launch_split_instance<16, 2>(src, op, stream);
+    else if (op.n <= 32) st = launch_split_instance<32, 2>(src, op, stream);
+    else st = launch_split_instance<64, 4>(src, op, stream);
+  } else {        // fused path (no scratch beyond the fallback list)
+    if (op.n <= 16) st = launch_trd_instance<16, 2>(src, op, stream);
+    else if (op.n <= 32) st = launch_trd_instance<32, 2>(src, op, stream);
+    else st = launch_trd_instance<64, 4>(src, op, stream);
+  }
   if (st != LLR_OK || op.block_stat) return st;
   BlockSource fb = src;
   fb.blk_list = op.fb_list;
