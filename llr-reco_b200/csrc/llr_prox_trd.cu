@@ -815,9 +815,19 @@ __global__ void __launch_bounds__(kEigThreads, 4) llr_eig_apply_kernel(BlockSour
   for (long long blk = blockIdx.x; blk < src.nblocks; blk += gridDim.x) {
     const long long base = src.kind == 1 ? 0 : blk * (long long)m * n;
     const float2* G = op.gram + blk * (long long)P;
-    for (int i = tid; i < P; i += blockDim.x) A[i] = G[i];
-    __syncthreads();
-    hermitian_tridiag<NPMAX, true>(A, n, trd, misc->red);
+    float fro = 0.f;   // ||G||_F^2 from the packed lower triangle
+    for (int i = tid; i < P; i += blockDim.x) {
+      const float2 v = G[i];
+      A[i] = v;
+      const int r = (int)((sqrtf(8.f * (float)i + 1.f) - 1.f) * 0.5f);
+      const int rr = (r * (r + 1) / 2 > i) ? r - 1 : ((r + 1) * (r + 2) / 2 <= i ? r + 1 : r);
+      fro += (i - rr * (rr + 1) / 2 == rr ? 1.f : 2.f) * cabs2(v);
+    }
+    fro = block_sum(fro, misc->red);
+    // lambda_max <= ||G||_F: below lambda^2 every singular value is shrunk to zero.
+    const bool all_zero = !op.block_stat && op.mode != LLR_PROX_HARD_RANK && op.lambda > 0.f &&
+                          fro <= op.lambda * op.lambda * op.lambda * op.lambda;
+    if (!all_zero) hermitian_tridiag<NPMAX, true>(A, n, trd, misc->red);
     if (op.block_stat) {
       tridiag_setup<NPMAX>(trd, n, LLR_PROX_HARD_RANK, 1, 0.f, misc);
       tridiag_eigenvalues<NPMAX>(trd, n, n - 1, 1, misc);
@@ -825,8 +835,12 @@ __global__ void __launch_bounds__(kEigThreads, 4) llr_eig_apply_kernel(BlockSour
       __syncthreads();
       continue;
     }
-    tridiag_setup<NPMAX>(trd, n, op.mode, op.rank, op.lambda, misc);
-    const int ra = misc->ra, nb = misc->n_below;
+    int ra = 0, nb = n;
+    if (!all_zero) {
+      tridiag_setup<NPMAX>(trd, n, op.mode, op.rank, op.lambda, misc);
+      ra = misc->ra;
+      nb = misc->n_below;
+    }
     if (ra == n && op.mode == LLR_PROX_HARD_RANK) {
       __syncthreads();
       continue;  // rank >= n: identity, nothing to write
