@@ -67,7 +67,8 @@ typedef struct llr_config {
   uint64_t seed;              /* key of the counter-based shift RNG                  */
   int32_t device;             /* CUDA device ordinal                                 */
   int32_t eig_solver;         /* 0: tridiagonal + bisection (default); 1: Jacobi      */
-  int32_t reserved[6];
+  int32_t gram_mode;          /* 0: 3xTF32 tensor cores (default); 1: FP32 FMA        */
+  int32_t reserved[5];
 } llr_config;
 
 /* ---- library / errors ------------------------------------------------------------ */

@@ -128,6 +128,13 @@ int make_plan(llr_ctx* c) {
 
 }  // namespace
 
+int check_device_error(llr_ctx* c) {
+  int h = 0;
+  LLR_CUDA_TRY(cudaMemcpy(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (h != 0) return set_error(LLR_ERR_CUDA, "a tensor-core wait in the prox kernel timed out (device flag %d)", h);
+  return LLR_OK;
+}
+
 PhaseTab ctx_phase(const llr_ctx* c, const float2* base, bool with_x) {
   PhaseTab t;
   t.x = with_x ? base : nullptr;
@@ -191,6 +198,8 @@ static int prox_pass(llr_ctx* c, cudaStream_t s, const int* explicit_shift, bool
     op.fb_list = c->d_fb;
     op.fb_count = c->d_fb + std::max<long long>(1, c->nblocks);
     op.gram = c->d_gram;
+    op.gram_mode = c->cfg.gram_mode;
+    op.err = c->d_err;
     LLR_TRY(launch_llr_prox(src, op, s));
   }
   if (block_stat || standalone) return LLR_OK;
@@ -288,6 +297,9 @@ int llr_ctx_create(const llr_config* cfg, llr_ctx** out) {
   if ((st = dalloc(&c->d_iter, 1))) return fail(st);
   if ((st = dalloc(&c->d_block_stat, (size_t)std::max<long long>(1, c->nblocks)))) return fail(st);
   if ((st = dalloc(&c->d_fb, (size_t)std::max<long long>(1, c->nblocks) + 1))) return fail(st);
+  if ((st = dalloc(&c->d_err, 1))) return fail(st);
+  e = cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream);
+  if (e != cudaSuccess) return fail(cuda_error(e, "cudaMemsetAsync", __FILE__, __LINE__));
   if (cfg->subspace_rank == 0 &&
       (st = dalloc(&c->d_gram, (size_t)std::max<long long>(1, c->nblocks) * ((size_t)c->g.nq * (c->g.nq + 1) / 2))))
     return fail(st);
@@ -324,7 +336,7 @@ int llr_ctx_destroy(llr_ctx* c) {
   if (c->have_plan) cufftDestroy(c->plan_fwd);
   dfree(c->d_x); dfree(c->d_work); dfree(c->d_yhat); dfree(c->d_samp_pos); dfree(c->d_samp_off);
   dfree(c->d_ph_ksp); dfree(c->d_ph_img); dfree(c->d_S); dfree(c->d_partials); dfree(c->d_hist); dfree(c->d_iter);
-  dfree(c->d_block_stat); dfree(c->d_fb); dfree(c->d_gram); dfree(c->d_wavelet_work); dfree(c->d_fft_work);
+  dfree(c->d_block_stat); dfree(c->d_fb); dfree(c->d_gram); dfree(c->d_err); dfree(c->d_wavelet_work); dfree(c->d_fft_work);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return LLR_OK;
@@ -692,6 +704,7 @@ int llr_iterate(llr_ctx* c, int32_t n, double* hist) {
                                    cudaMemcpyDeviceToHost, c->stream));
   }
   LLR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  LLR_TRY(llr::check_device_error(c));
   if (hist && n > 0) {
     const long long lo = std::max<long long>(0, it0), hi = std::min<long long>(c->hist_cap, it0 + n);
     for (long long i = lo; i < hi; ++i)

@@ -189,6 +189,7 @@ int llr_config_validate(const llr_config* c) {
     return set_error(LLR_ERR_INVALID, "llr rank must be <= subspace rank (lib.rs:217)");
   if (!(c->wavelet_alpha >= 0.f)) return set_error(LLR_ERR_INVALID, "wavelet_alpha must be >= 0");
   if (c->eig_solver != 0 && c->eig_solver != 1) return set_error(LLR_ERR_INVALID, "eig_solver must be 0 or 1");
+  if (c->gram_mode != 0 && c->gram_mode != 1) return set_error(LLR_ERR_INVALID, "gram_mode must be 0 or 1");
   if (c->wavelet_alpha > 0.f && (c->wavelet_moments < 1 || c->wavelet_moments > 10))
     return set_error(LLR_ERR_INVALID, "wavelet_moments must be in [1, 10]");
   if (m < 1) return set_error(LLR_ERR_INVALID, "empty block");
@@ -366,6 +367,8 @@ static int batch_prox(int m, int n, int mode, int rank, float lam, int batch, ll
   op.fb_list = fb;
   op.fb_count = fb + batch;
   op.gram = gram;
+  op.gram_mode = 0;
+  op.err = nullptr;
   int st = launch_llr_prox(src, op, s);
   e = cudaFreeAsync(fb, s);
   cudaError_t e2 = cudaFreeAsync(gram, s);

@@ -1,0 +1,320 @@
+// Gram matrices of the LLR blocks on the 5th-generation tensor cores (tcgen05).
+//
+// For a Casorati block C (m x n complex) let D = [Re C | Im C] (m x 2n real).  Then
+// P = D^T D (2n x 2n) gives G = C^H C as
+//   Re G[i][j] = P[i][j] + P[n+i][n+j],   Im G[i][j] = P[i][n+j] - P[n+i][j].
+// P is one 128 x 128 UMMA accumulator in tensor memory (2n <= 128), K = the m voxel rows.
+// Both operands are the same shared-memory tile of D in the K-major, no-swizzle canonical
+// layout (8-row x 16-byte core matrices), so A = B and the MMA computes D^T D directly.
+// Precision: 3xTF32 -- x = hi + lo with hi = tf32(x), and P accumulates hi*hi + hi*lo + lo*hi
+// in FP32, which keeps FP32-level accuracy (the lo*lo term is below FP32 rounding).
+// Rows stream in 32-row chunks, double-buffered: while the tensor core consumes one chunk the
+// 128 threads gather, phase-correct and split the next one.  One elected thread issues the
+// MMAs and commits them to an mbarrier; every wait is bounded and reports a timeout through
+// op.err instead of hanging.
+#include <cstdio>
+#include <algorithm>
+
+#include "llr_prox_common.cuh"
+
+namespace llr {
+
+namespace {
+
+constexpr int kTcThreads = 128;
+constexpr int kKC = 32;                    // rows (K) per staged chunk
+constexpr int kKB = kKC / 4;               // 16-byte K groups per chunk
+constexpr int kOpBytes = 128 * kKC * 4;    // one operand plane (hi or lo) of one chunk
+constexpr unsigned long long kWaitLimit = 1ull << 22;   // bounded spin: ~seconds, never forever
+
+struct TcRowTab {
+  int off;
+  int cx;
+  int cyz;
+  int pad;
+};
+
+struct TcLayout {
+  size_t off_hdr, off_row, off_rowph, off_op, total;
+  int op_bytes;        // bytes of the operand / P-staging region
+};
+
+struct TcHdr {
+  unsigned long long mbar[3];   // chunk buffer 0, chunk buffer 1, block done
+  unsigned int tmem;            // tensor-memory base address
+  int shift[3];
+  int fail;
+  int pad;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// K-major, no-swizzle UMMA shared-memory descriptor (sm_100 version 1).
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;
+  return d;
+}
+
+// Instruction descriptor: TF32 x TF32 -> F32, both K-major, M = 128, N = 128.
+constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
+
+__device__ __forceinline__ void umma_tf32(uint32_t d, uint64_t a, uint64_t b, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+      "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t mbar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, P1;\n\t}" : "=r"(ok) : "r"(mbar), "r"(parity) : "memory");
+  return ok != 0;
+}
+
+// Bounded wait; returns false when the limit runs out.
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+  for (unsigned long long i = 0; i < kWaitLimit; ++i)
+    if (mbar_try(mbar, parity)) return true;
+  return false;
+}
+
+__device__ __forceinline__ uint32_t tf32_rna(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+
+// Element (mn, k) of one operand plane: core matrix (mn/8, k/4) of 8 rows x 16 bytes.
+__device__ __forceinline__ int op_offset(int mn, int kb) { return ((mn >> 3) * kKB + kb) * 128 + (mn & 7) * 16; }
+
+template <int NPMAX>
+__global__ void __launch_bounds__(kTcThreads, 2) llr_gram_tc_kernel(BlockSource src, ProxOp op, TcLayout L) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  TcHdr* hdr = reinterpret_cast<TcHdr*>(smem + L.off_hdr);
+  TcRowTab* rows = reinterpret_cast<TcRowTab*>(smem + L.off_row);
+  float2* rowph = reinterpret_cast<float2*>(smem + L.off_rowph);
+  unsigned char* ops = smem + L.off_op;   // [buf][hi, lo] planes; reused as P staging
+  const int m = op.m, n = op.n, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const long long qstride = src.kind == 1 ? src.g.V : (long long)m;
+  const long long Pn = (long long)n * (n + 1) / 2;
+  const int nchunks = (m + kKC - 1) / kKC;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&hdr->tmem)),
+                 "r"(128u));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    for (int b = 0; b < 3; ++b)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&hdr->mbar[b])));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+    block_shift(src, hdr->shift);
+    hdr->fail = 0;
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = hdr->tmem;
+  const int sh[3] = {hdr->shift[0], hdr->shift[1], hdr->shift[2]};
+  uint32_t phase[3] = {0u, 0u, 0u};
+  bool used[2] = {false, false};
+  bool failed = false;
+
+  for (long long blk = blockIdx.x; blk < src.nblocks && !failed; blk += gridDim.x) {
+    const long long base = src.kind == 1 ? 0 : blk * (long long)m * n;
+    for (int r = tid; r < m; r += kTcThreads) {
+      TcRowTab rt;
+      if (src.kind == 1) {
+        int ix, iy, iz;
+        block_row_coord(src, blk, sh, r, ix, iy, iz);
+        rt.off = (int)planar_index(src.g, ix, iy, iz, 0);
+        rt.cx = ix;
+        rt.cyz = iy | (iz << 16);
+        if (src.ph_uniform) rowph[r] = phase_at(src.ph, src.g, 0, ix, iy, iz);
+      } else {
+        rt.off = r;
+        rt.cx = 0;
+        rt.cyz = 0;
+      }
+      rt.pad = 0;
+      rows[r] = rt;
+    }
+    // operand planes start zeroed (rows 2n..127 and K padding must contribute nothing)
+    for (int i = tid; i < 4 * kOpBytes / 16; i += kTcThreads)
+      reinterpret_cast<float4*>(ops)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    __syncthreads();
+
+    for (int c = 0; c < nchunks; ++c) {
+      const int b = c & 1;
+      if (used[b]) {  // the MMAs that read this buffer two chunks ago must be done
+        const bool ok = mbar_wait(smem_u32(&hdr->mbar[b]), phase[b]);
+        phase[b] ^= 1u;
+        if (__syncthreads_or(!ok)) { failed = true; break; }
+      }
+      unsigned char* hi = ops + (size_t)b * 2 * kOpBytes;
+      unsigned char* lo = hi + kOpBytes;
+      const int c0 = c * kKC;
+      // task (kb, q): rows c0 + 4kb .. +3 of column q -> one 16-byte group of each plane
+      for (int task = tid; task < kKB * n; task += kTcThreads) {
+        const int kb = task / n, q = task - kb * n;
+        float2 v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int r = c0 + 4 * kb + u;
+          v[u] = make_float2(0.f, 0.f);
+          if (r < m) {
+            const TcRowTab rt = rows[r];
+            float2 x = src.data[base + (long long)rt.off + (long long)q * qstride];
+            if (src.kind == 1) {
+              float2 p;
+              if (src.ph_uniform) p = rowph[r];
+              else p = phase_at(src.ph, src.g, q, rt.cx, rt.cyz & 0xffff, rt.cyz >> 16);
+              x = cscale(cmul_bc(x, p), src.load_scale);
+            }
+            v[u] = x;
+          }
+        }
+        uint4 rh, ih, rl, il;
+        uint32_t* prh = &rh.x; uint32_t* pih = &ih.x; uint32_t* prl = &rl.x; uint32_t* pil = &il.x;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const uint32_t a = tf32_rna(v[u].x), bb = tf32_rna(v[u].y);
+          prh[u] = a;
+          pih[u] = bb;
+          prl[u] = __float_as_uint(v[u].x - __uint_as_float(a));
+          pil[u] = __float_as_uint(v[u].y - __uint_as_float(bb));
+        }
+        *reinterpret_cast<uint4*>(hi + op_offset(q, kb)) = rh;
+        *reinterpret_cast<uint4*>(hi + op_offset(n + q, kb)) = ih;
+        *reinterpret_cast<uint4*>(lo + op_offset(q, kb)) = rl;
+        *reinterpret_cast<uint4*>(lo + op_offset(n + q, kb)) = il;
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncthreads();
+      if (tid == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        const uint32_t ah = smem_u32(hi), al = smem_u32(lo);
+#pragma unroll
+        for (int s = 0; s < kKC / 8; ++s) {
+          const uint64_t dh = umma_desc(ah + s * 256, 128, kKB * 128);
+          const uint64_t dl = umma_desc(al + s * 256, 128, kKB * 128);
+          umma_tf32(tmem, dh, dh, (c > 0 || s > 0) ? 1u : 0u);
+          umma_tf32(tmem, dh, dl, 1u);
+          umma_tf32(tmem, dl, dh, 1u);
+        }
+        umma_commit(smem_u32(&hdr->mbar[b]));
+        if (c == nchunks - 1) umma_commit(smem_u32(&hdr->mbar[2]));
+      }
+      used[b] = true;
+    }
+    if (failed) break;
+    // all MMAs of this block complete -> read P and stage it in the (now idle) operand area
+    {
+      const bool ok = mbar_wait(smem_u32(&hdr->mbar[2]), phase[2]);
+      phase[2] ^= 1u;
+      // the done barrier implies every chunk barrier's MMAs finished too; consume them
+      for (int bb = 0; bb < 2; ++bb)
+        if (used[bb]) {
+          mbar_wait(smem_u32(&hdr->mbar[bb]), phase[bb]);
+          phase[bb] ^= 1u;
+          used[bb] = false;
+        }
+      if (__syncthreads_or(!ok)) { failed = true; break; }
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    float* Ps = reinterpret_cast<float*>(ops);
+    const int ldp = 2 * n + 1;
+    const int a = 32 * warp + lane;          // accumulator row held by this thread
+    for (int cc = 0; cc < 2 * n; cc += 32) {
+      uint32_t r[32];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+          "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+            "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+            "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+          : "r"(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)cc));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (a < 2 * n) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j)
+          if (cc + j < 2 * n) Ps[a * ldp + cc + j] = __uint_as_float(r[j]);
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    float2* G = op.gram + blk * Pn;
+    for (long long idx = tid; idx < Pn; idx += kTcThreads) {
+      const int i = (int)((sqrtf(8.f * (float)idx + 1.f) - 1.f) * 0.5f);
+      const int ii = ((long long)i * (i + 1) / 2 > idx) ? i - 1 : (((long long)(i + 1) * (i + 2) / 2 <= idx) ? i + 1 : i);
+      const int j = (int)(idx - (long long)ii * (ii + 1) / 2);
+      const float re = Ps[ii * ldp + j] + Ps[(n + ii) * ldp + n + j];
+      const float im = Ps[ii * ldp + n + j] - Ps[(n + ii) * ldp + j];
+      G[idx] = make_float2(re, im);
+    }
+    __syncthreads();
+  }
+
+  if (failed && tid == 0 && op.err) atomicExch(op.err, 1);
+  // make sure nothing is still writing the accumulator before it is released
+  if (tid == 0) {
+    umma_commit(smem_u32(&hdr->mbar[2]));
+  }
+  mbar_wait(smem_u32(&hdr->mbar[2]), phase[2]);
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128u));
+}
+
+template <int NPMAX>
+TcLayout make_tc_layout(int m, int n) {
+  TcLayout L;
+  size_t off = 0;
+  L.off_hdr = off; off = align16(off + sizeof(TcHdr));
+  L.off_row = off; off = align16(off + sizeof(TcRowTab) * (size_t)m);
+  L.off_rowph = off; off = align16(off + sizeof(float2) * (size_t)m);
+  off = (off + 1023) & ~size_t(1023);
+  L.off_op = off;
+  const size_t opb = std::max<size_t>(4 * (size_t)kOpBytes, sizeof(float) * (size_t)(2 * n) * (2 * n + 1));
+  L.op_bytes = (int)opb;
+  off += opb;
+  L.total = off;
+  return L;
+}
+
+}  // namespace
+
+bool llr_gram_tc_supported(int m, int n) {
+  if (n < 1 || 2 * n > 128 || m < 1) return false;
+  return make_tc_layout<64>(m, n).total <= 227 * 1024;
+}
+
+int launch_llr_gram_tc(const BlockSource& src, const ProxOp& op, cudaStream_t stream) {
+  if (2 * op.n > 128) return set_error(LLR_ERR_UNSUPPORTED, "tensor-core Gram needs 2n <= 128 (n = %d)", op.n);
+  TcLayout L = make_tc_layout<64>(op.m, op.n);
+  if (L.total > 227 * 1024) return set_error(LLR_ERR_UNSUPPORTED, "tensor-core Gram needs %zu B smem", L.total);
+  auto kern = llr_gram_tc_kernel<64>;
+  LLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total));
+  int dev = 0, nsm = 0, occ = 0;
+  LLR_CUDA_TRY(cudaGetDevice(&dev));
+  LLR_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  LLR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kTcThreads, L.total));
+  if (occ < 1) return set_error(LLR_ERR_UNSUPPORTED, "tensor-core Gram kernel cannot be resident");
+  occ = std::min(occ, 4);  // 128 TMEM columns per CTA, 512 per SM
+  const long long grid = std::min<long long>(src.nblocks, (long long)nsm * occ);
+  if (grid < 1) return LLR_OK;
+  kern<<<(unsigned)grid, kTcThreads, L.total, stream>>>(src, op, L);
+  LLR_CUDA_TRY(cudaGetLastError());
+  return LLR_OK;
+}
+
+}  // namespace llr

@@ -43,10 +43,14 @@ struct ProxOp {
   int* fb_list;        // blocks handed to the Jacobi kernel (capacity nblocks)
   int* fb_count;
   float2* gram;        // optional scratch, nblocks * n(n+1)/2: selects the split Gram/eigen path
+  int gram_mode;       // 0: 3xTF32 on tensor cores (tcgen05) where 2n <= 128; 1: FP32 FMA
+  int* err;            // device flag set when a bounded wait gives up (never expected)
 };
 
 int launch_llr_prox(const BlockSource& src, const ProxOp& op, cudaStream_t stream);
 bool llr_prox_supported(int m, int n);
+bool llr_gram_tc_supported(int m, int n);
+int launch_llr_gram_tc(const BlockSource& src, const ProxOp& op, cudaStream_t stream);
 
 struct SubspaceOp {
   int m, nq, srank;
@@ -122,6 +126,7 @@ struct llr_ctx {
   float* d_block_stat;
   int* d_fb;                // Jacobi fallback block list (nblocks) + count
   float2* d_gram;           // per-block packed Gram matrices (split prox path)
+  int* d_err;               // device error flag of the prox kernels
   int ph_uniform;           // all volumes share the image-domain phase tables
   float2* d_wavelet_work;
   size_t wavelet_work_elems;
@@ -147,5 +152,6 @@ struct llr_ctx {
 namespace llr {
 int ctx_enqueue_iteration(llr_ctx* ctx, cudaStream_t s);
 int ctx_prox(llr_ctx* ctx, cudaStream_t s, const int* explicit_shift, float* block_stat);
+int check_device_error(llr_ctx* ctx);
 PhaseTab ctx_phase(const llr_ctx* ctx, const float2* base, bool with_x);
 }

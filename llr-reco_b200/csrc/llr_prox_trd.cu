@@ -908,7 +908,9 @@ int launch_split_instance(const BlockSource& src, const ProxOp& op, cudaStream_t
   int dev = 0, nsm = 0, occ = 0;
   LLR_CUDA_TRY(cudaGetDevice(&dev));
   LLR_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  {
+  if (op.gram_mode == 0 && llr_gram_tc_supported(op.m, op.n)) {
+    LLR_TRY(launch_llr_gram_tc(src, op, stream));
+  } else {
     TrdLayout L = make_trd_layout<NPMAX, TG>(op.m, op.n);
     auto kern = llr_gram_kernel<NPMAX, TG>;
     LLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total));

@@ -54,7 +54,8 @@ class llr_config(C.Structure):
         ("seed", C.c_uint64),
         ("device", C.c_int32),
         ("eig_solver", C.c_int32),
-        ("reserved", C.c_int32 * 6),
+        ("gram_mode", C.c_int32),
+        ("reserved", C.c_int32 * 5),
     ]
 
 

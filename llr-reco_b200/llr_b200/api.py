@@ -115,6 +115,7 @@ class ReconParams:
     seed: int = 0
     device: int = 0
     eig_solver: int = 0
+    gram_mode: int = 0
 
     def to_c(self) -> L.llr_config:
         c = L.llr_config()
@@ -134,6 +135,7 @@ class ReconParams:
         c.seed = int(self.seed)
         c.device = int(self.device)
         c.eig_solver = int(self.eig_solver)
+        c.gram_mode = int(self.gram_mode)
         return c
 
 

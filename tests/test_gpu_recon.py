@@ -30,7 +30,7 @@ def oracle_cfg(bs, mode, rank=0, lam=0.0, seed=0, **kw):
 
 
 def run_both(y, bs, mode, n_iter, rank=2, lam_rel=0.02, seed=5, lin=None, wavelet=None, subspace=None,
-             max_shift=None, eig_solver=0):
+             max_shift=None, eig_solver=0, gram_mode=0):
     nx, ny, nz, nq = y.shape
     ocfg = oracle_cfg(bs, "hard" if mode == L.LLR_PROX_HARD_RANK else "soft", rank=rank, seed=seed,
                       max_rand_shift=max_shift)
@@ -46,7 +46,7 @@ def run_both(y, bs, mode, n_iter, rank=2, lam_rel=0.02, seed=5, lin=None, wavele
     if wavelet is not None:
         ocfg.wavelet_alpha, ocfg.wavelet_moments, ocfg.wavelet_levels = wavelet
     p = ReconParams(vol_size=(nx, ny, nz), nq=nq, block_size=bs, prox_mode=mode, rank=rank, lam=lam, seed=seed,
-                    max_rand_shift=max_shift, eig_solver=eig_solver,
+                    max_rand_shift=max_shift, eig_solver=eig_solver, gram_mode=gram_mode,
                     subspace_rank=0 if subspace is None else subspace.shape[1])
     if wavelet is not None:
         p.wavelet_alpha, p.wavelet_moments, p.wavelet_levels = wavelet
@@ -88,12 +88,14 @@ def test_hard_rank_c1_like(gpu, eig_solver):
     check(gx, ox, gh, oh)
 
 
-@pytest.mark.parametrize("eig_solver", [0, 1])
-def test_soft_c2_like(gpu, eig_solver):
+@pytest.mark.parametrize("eig_solver,gram_mode", [(0, 0), (1, 0), (0, 1)])
+def test_soft_c2_like(gpu, eig_solver, gram_mode):
     """Config-2 shape class: 6^3 blocks, 61 volumes (Casorati 216 x 61), reduced volume; both
-    eigen-solvers (tridiagonal + bisection, Jacobi)."""
+    eigen-solvers (tridiagonal + bisection, Jacobi) and both Gram paths (3xTF32 tensor cores,
+    FP32 FMA)."""
     d = dataset((24, 24, 12), 61, accel=8.0, centre=6)
-    gx, ox, gh, oh, _ = run_both(d.y, (6, 6, 6), L.LLR_PROX_SOFT_THRESH, 4, eig_solver=eig_solver)
+    gx, ox, gh, oh, _ = run_both(d.y, (6, 6, 6), L.LLR_PROX_SOFT_THRESH, 4, eig_solver=eig_solver,
+                                 gram_mode=gram_mode)
     check(gx, ox, gh, oh)
 
 
