@@ -152,6 +152,24 @@ __global__ void __launch_bounds__(kTcThreads, 2) llr_gram_tc_kernel(BlockSource 
       reinterpret_cast<float4*>(ops)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     __syncthreads();
 
+    // Register prefetch: each thread owns up to kTasks (kb, q) tasks of a chunk, 4 rows each.
+    constexpr int kTasks = 4;
+    float2 pre[kTasks][4];
+    auto load_chunk = [&](int c) {
+      const int c0 = c * kKC;
+#pragma unroll
+      for (int t = 0; t < kTasks; ++t) {
+        const int task = tid + t * kTcThreads;
+        const int kb = task / n, q = task - kb * n;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int r = c0 + 4 * kb + u;
+          pre[t][u] = make_float2(0.f, 0.f);
+          if (task < kKB * n && r < m) pre[t][u] = src.data[base + (long long)rows[r].off + (long long)q * qstride];
+        }
+      }
+    };
+    load_chunk(0);
     for (int c = 0; c < nchunks; ++c) {
       const int b = c & 1;
       if (used[b]) {  // the MMAs that read this buffer two chunks ago must be done
@@ -162,41 +180,38 @@ __global__ void __launch_bounds__(kTcThreads, 2) llr_gram_tc_kernel(BlockSource 
       unsigned char* hi = ops + (size_t)b * 2 * kOpBytes;
       unsigned char* lo = hi + kOpBytes;
       const int c0 = c * kKC;
-      // task (kb, q): rows c0 + 4kb .. +3 of column q -> one 16-byte group of each plane
-      for (int task = tid; task < kKB * n; task += kTcThreads) {
-        const int kb = task / n, q = task - kb * n;
-        float2 v[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int r = c0 + 4 * kb + u;
-          v[u] = make_float2(0.f, 0.f);
-          if (r < m) {
-            const TcRowTab rt = rows[r];
-            float2 x = src.data[base + (long long)rt.off + (long long)q * qstride];
-            if (src.kind == 1) {
-              float2 p;
-              if (src.ph_uniform) p = rowph[r];
-              else p = phase_at(src.ph, src.g, q, rt.cx, rt.cyz & 0xffff, rt.cyz >> 16);
-              x = cscale(cmul_bc(x, p), src.load_scale);
-            }
-            v[u] = x;
-          }
-        }
+      for (int t = 0; t < kTasks; ++t) {
+        const int task = tid + t * kTcThreads;
+        if (task >= kKB * n) continue;
+        const int kb = task / n, q = task - kb * n;
         uint4 rh, ih, rl, il;
         uint32_t* prh = &rh.x; uint32_t* pih = &ih.x; uint32_t* prl = &rl.x; uint32_t* pil = &il.x;
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-          const uint32_t a = tf32_rna(v[u].x), bb = tf32_rna(v[u].y);
+          const int r = c0 + 4 * kb + u;
+          float2 x = pre[t][u];
+          if (src.kind == 1 && r < m) {
+            float2 p;
+            if (src.ph_uniform) p = rowph[r];
+            else {
+              const TcRowTab rt = rows[r];
+              p = phase_at(src.ph, src.g, q, rt.cx, rt.cyz & 0xffff, rt.cyz >> 16);
+            }
+            x = cscale(cmul_bc(x, p), src.load_scale);
+          }
+          const uint32_t a = tf32_rna(x.x), bb = tf32_rna(x.y);
           prh[u] = a;
           pih[u] = bb;
-          prl[u] = __float_as_uint(v[u].x - __uint_as_float(a));
-          pil[u] = __float_as_uint(v[u].y - __uint_as_float(bb));
+          prl[u] = __float_as_uint(x.x - __uint_as_float(a));
+          pil[u] = __float_as_uint(x.y - __uint_as_float(bb));
         }
         *reinterpret_cast<uint4*>(hi + op_offset(q, kb)) = rh;
         *reinterpret_cast<uint4*>(hi + op_offset(n + q, kb)) = ih;
         *reinterpret_cast<uint4*>(lo + op_offset(q, kb)) = rl;
         *reinterpret_cast<uint4*>(lo + op_offset(n + q, kb)) = il;
       }
+      if (c + 1 < nchunks) load_chunk(c + 1);   // in flight while the tensor core works
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncthreads();
       if (tid == 0) {
@@ -294,7 +309,7 @@ TcLayout make_tc_layout(int m, int n) {
 }  // namespace
 
 bool llr_gram_tc_supported(int m, int n) {
-  if (n < 1 || 2 * n > 128 || m < 1) return false;
+  if (n < 1 || 2 * n > 128 || m < 1 || 8 * n > 4 * kTcThreads) return false;
   return make_tc_layout<64>(m, n).total <= 227 * 1024;
 }
 
@@ -304,6 +319,7 @@ int launch_llr_gram_tc(const BlockSource& src, const ProxOp& op, cudaStream_t st
   if (L.total > 227 * 1024) return set_error(LLR_ERR_UNSUPPORTED, "tensor-core Gram needs %zu B smem", L.total);
   auto kern = llr_gram_tc_kernel<64>;
   LLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total));
+  LLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   int dev = 0, nsm = 0, occ = 0;
   LLR_CUDA_TRY(cudaGetDevice(&dev));
   LLR_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));

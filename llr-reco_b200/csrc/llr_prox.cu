@@ -106,6 +106,7 @@ int launch_jacobi_instance(const BlockSource& src, const ProxOp& op, cudaStream_
                      L.total);
   auto kern = llr_prox_jacobi_kernel<NPMAX, TG>;
   LLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total));
+    LLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   int dev = 0, nsm = 0, occ = 0;
   LLR_CUDA_TRY(cudaGetDevice(&dev));
   LLR_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
@@ -242,6 +243,7 @@ int launch_llr_prox_subspace(const BlockSource& src, const SubspaceOp& op, cudaS
   if (L.total > 227 * 1024) return set_error(LLR_ERR_UNSUPPORTED, "subspace prox needs %zu B smem", L.total);
   auto kern = llr_subspace_kernel<16>;
   LLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total));
+    LLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   int dev = 0, nsm = 0, occ = 0;
   LLR_CUDA_TRY(cudaGetDevice(&dev));
   LLR_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));

@@ -733,6 +733,7 @@ int launch_trd_instance(const BlockSource& src, const ProxOp& op, cudaStream_t s
     return set_error(LLR_ERR_UNSUPPORTED, "Casorati %dx%d needs %zu B of shared memory", op.m, op.n, L.total);
   auto kern = llr_prox_trd_kernel<NPMAX, TG>;
   LLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total));
+    LLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   int dev = 0, nsm = 0, occ = 0;
   LLR_CUDA_TRY(cudaGetDevice(&dev));
   LLR_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
@@ -914,6 +915,7 @@ int launch_split_instance(const BlockSource& src, const ProxOp& op, cudaStream_t
     TrdLayout L = make_trd_layout<NPMAX, TG>(op.m, op.n);
     auto kern = llr_gram_kernel<NPMAX, TG>;
     LLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total));
+    LLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     LLR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kLlrThreads, L.total));
     if (occ < 1) return set_error(LLR_ERR_UNSUPPORTED, "Gram kernel cannot be resident (smem %zu B)", L.total);
     const long long grid = std::min<long long>(src.nblocks, (long long)nsm * occ);
@@ -924,6 +926,7 @@ int launch_split_instance(const BlockSource& src, const ProxOp& op, cudaStream_t
     EigLayout L = make_eig_layout<NPMAX>(op.m);
     auto kern = llr_eig_apply_kernel<NPMAX>;
     LLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total));
+    LLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     LLR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kEigThreads, L.total));
     if (occ < 1) return set_error(LLR_ERR_UNSUPPORTED, "eigen kernel cannot be resident (smem %zu B)", L.total);
     const long long grid = std::min<long long>(src.nblocks, (long long)nsm * occ);
