@@ -130,6 +130,9 @@ int llr_iterate_async(llr_ctx* ctx, int32_t n_iter);
 int llr_iterate_profiled(llr_ctx* ctx, int32_t n_iter, double* stage_ms, double* total_ms);
 /* Device time of n single-graph iterations (events on the context stream). */
 int llr_iterate_timed(llr_ctx* ctx, int32_t n_iter, double* total_ms);
+/* Number of this library's kernels that one captured iteration launches (cuFFT's kernels
+ * are not counted).  Valid after the first llr_iterate* call; no reference counterpart. */
+int llr_ctx_kernel_launches(const llr_ctx* ctx, int32_t* per_iteration);
 int llr_get_iteration(const llr_ctx* ctx, int64_t* it);
 int llr_set_iteration(llr_ctx* ctx, int64_t it);
 /* Residual history of the last `count` iterations ending at the current one. */

@@ -551,7 +551,9 @@ static int build_graph(llr_ctx* c) {
   drop_graph(c);
   cudaStream_t s = c->stream;
   LLR_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  const long long n0 = launch_counter;
   int st = ctx_enqueue_iteration(c, s);
+  c->launches_per_iter = (int)(launch_counter - n0);
   cudaGraph_t graph = nullptr;
   cudaError_t e = cudaStreamEndCapture(s, &graph);
   if (st != LLR_OK) {
@@ -606,6 +608,7 @@ int llr_iterate_profiled(llr_ctx* c, int32_t n, double* stage_ms, double* total_
   if (c->cfg.subspace_rank > 0 && !c->d_S) return set_error(LLR_ERR_STATE, "subspace not uploaded");
   LLR_CUDA_TRY(cudaSetDevice(c->device));
   if (!c->have_stages) {
+    const long long n0 = launch_counter;
     for (int i = 0; i < 5; ++i) {
       int st = capture_stage(c, i, &c->stage_exec[i]);
       if (st != LLR_OK) {
@@ -614,6 +617,7 @@ int llr_iterate_profiled(llr_ctx* c, int32_t n, double* stage_ms, double* total_
       }
     }
     c->have_stages = true;
+    c->launches_per_iter = (int)(launch_counter - n0);
   }
   std::vector<cudaEvent_t> ev((size_t)n * 6, nullptr);
   int st = LLR_OK;
@@ -711,6 +715,13 @@ int llr_iterate(llr_ctx* c, int32_t n, double* hist) {
       if (!std::isfinite(hist[i - it0]))
         return set_error(LLR_ERR_NOT_FINITE, "non-finite data-consistency residual at iteration %lld", i);
   }
+  return LLR_OK;
+}
+
+int llr_ctx_kernel_launches(const llr_ctx* c, int32_t* per_iteration) {
+  if (!c || !per_iteration) return set_error(LLR_ERR_INVALID, "null pointer");
+  if (!c->have_graph && !c->have_stages) return set_error(LLR_ERR_STATE, "no iteration has been captured yet");
+  *per_iteration = c->launches_per_iter;
   return LLR_OK;
 }
 

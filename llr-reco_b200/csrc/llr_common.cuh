@@ -15,6 +15,12 @@ namespace llr {
 int set_error(int status, const char* fmt, ...);
 int cuda_error(cudaError_t e, const char* what, const char* file, int line);
 
+// Kernel launches issued by the calling thread. Every launch site of the library calls
+// note_launch() just before its launch; the iteration graph builder reads the difference
+// across its capture to know how many of the library's kernels one iteration runs.
+inline thread_local long long launch_counter = 0;
+inline void note_launch() { ++launch_counter; }
+
 }  // namespace llr
 
 #define LLR_CUDA_TRY(expr)                                                         \

@@ -320,14 +320,26 @@ int launch_llr_gram_tc(const BlockSource& src, const ProxOp& op, cudaStream_t st
   auto kern = llr_gram_tc_kernel<64>;
   LLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total));
   LLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-  int dev = 0, nsm = 0, occ = 0;
+  int dev = 0, nsm = 0, smem_sm = 0, regs_sm = 0;
   LLR_CUDA_TRY(cudaGetDevice(&dev));
   LLR_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  LLR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kTcThreads, L.total));
+  LLR_CUDA_TRY(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+  LLR_CUDA_TRY(cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev));
+  cudaFuncAttributes fa{};
+  LLR_CUDA_TRY(cudaFuncGetAttributes(&fa, kern));
+  // Residency from the kernel's own resources. The occupancy query reports one CTA per SM for
+  // this kernel although three fit, so the count is derived here: shared memory (the driver
+  // reserves 1 KB per CTA), registers (allocated per warp in units of 256) and TMEM (128 of
+  // the SM's 512 columns per CTA). The kernel strides over blocks, so a grid larger than
+  // what is resident is still correct, only slower.
+  const int regs_warp = ((fa.numRegs * 32 + 255) / 256) * 256;
+  const int by_regs = regs_warp > 0 ? regs_sm / (regs_warp * (kTcThreads / 32)) : 4;
+  const int by_smem = smem_sm / (int)(L.total + fa.sharedSizeBytes + 1024);
+  int occ = std::min(std::min(by_regs, by_smem), 4);
   if (occ < 1) return set_error(LLR_ERR_UNSUPPORTED, "tensor-core Gram kernel cannot be resident");
-  occ = std::min(occ, 4);  // 128 TMEM columns per CTA, 512 per SM
   const long long grid = std::min<long long>(src.nblocks, (long long)nsm * occ);
   if (grid < 1) return LLR_OK;
+  note_launch();
   kern<<<(unsigned)grid, kTcThreads, L.total, stream>>>(src, op, L);
   LLR_CUDA_TRY(cudaGetLastError());
   return LLR_OK;

@@ -143,6 +143,7 @@ struct llr_ctx {
   bool have_graph;
   cudaGraphExec_t stage_exec[5];
   bool have_stages;
+  int launches_per_iter;   // library kernels one iteration launches (counted at capture)
   // measurement stats
   double total_energy;
   double undersampling;

@@ -114,6 +114,7 @@ int launch_jacobi_instance(const BlockSource& src, const ProxOp& op, cudaStream_
   if (occ < 1) return set_error(LLR_ERR_UNSUPPORTED, "prox kernel cannot be resident (smem %zu B)", L.total);
   long long grid = std::min<long long>(src.nblocks, (long long)nsm * occ);
   if (grid < 1) return LLR_OK;
+  note_launch();
   kern<<<(unsigned)grid, kLlrThreads, L.total, stream>>>(src, op, L);
   LLR_CUDA_TRY(cudaGetLastError());
   return LLR_OK;
@@ -250,6 +251,7 @@ int launch_llr_prox_subspace(const BlockSource& src, const SubspaceOp& op, cudaS
   LLR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kLlrThreads, L.total));
   if (occ < 1) return set_error(LLR_ERR_UNSUPPORTED, "subspace kernel cannot be resident");
   long long grid = std::min<long long>(src.nblocks, (long long)nsm * occ);
+  note_launch();
   kern<<<(unsigned)grid, kLlrThreads, L.total, stream>>>(src, op, L);
   LLR_CUDA_TRY(cudaGetLastError());
   return LLR_OK;
@@ -297,6 +299,7 @@ int launch_lift(const float2* vol, float2* mat, const int* vs, int nq, const int
   const long long tot = (long long)bs[0] * bs[1] * bs[2] * nq * n;
   if (tot == 0) return LLR_OK;
   long long blocks = std::min<long long>((tot + 255) / 256, 148LL * 16);
+  note_launch();
   lift_kernel<<<(unsigned)blocks, 256, 0, s>>>(vol, mat, vs[0], vs[1], vs[2], nq, bs[0], bs[1], bs[2], g[0], g[1],
                                                sh[0], sh[1], sh[2], start, n, dir);
   LLR_CUDA_TRY(cudaGetLastError());
@@ -378,6 +381,7 @@ __global__ void conj_transpose_kernel(const float2* __restrict__ in, float2* __r
 int launch_conj_transpose(const float2* in, float2* out, int m, int n, int batch, cudaStream_t s) {
   if ((long long)m * n * batch == 0) return LLR_OK;
   dim3 grid((m + 31) / 32, (n + 31) / 32, batch);
+  note_launch();
   conj_transpose_kernel<<<grid, dim3(32, 8), 0, s>>>(in, out, m, n);
   LLR_CUDA_TRY(cudaGetLastError());
   return LLR_OK;
@@ -387,6 +391,7 @@ int launch_rhs_cdgmm(int m, int n, int batch, float2* a, const float* d, cudaStr
   const long long tot = (long long)m * n * batch;
   if (tot == 0) return LLR_OK;
   long long blocks = std::min<long long>((tot + 255) / 256, 148LL * 32);
+  note_launch();
   rhs_cdgmm_kernel<<<(unsigned)blocks, 256, 0, s>>>(m, n, batch, a, d);
   LLR_CUDA_TRY(cudaGetLastError());
   return LLR_OK;
@@ -397,6 +402,7 @@ int launch_cgemm(int m, int k, int n, int batch, int broadcast_a, float2 alpha, 
   if (m == 0 || n == 0 || batch == 0) return LLR_OK;
   dim3 grid((m + 15) / 16, (n + 15) / 16, batch);
   dim3 block(16, 16);
+  note_launch();
   cgemm_kernel<<<grid, block, 0, s>>>(m, k, n, broadcast_a, alpha, beta, ta, tb, A, B, C);
   LLR_CUDA_TRY(cudaGetLastError());
   return LLR_OK;

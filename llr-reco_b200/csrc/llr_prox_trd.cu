@@ -741,6 +741,7 @@ int launch_trd_instance(const BlockSource& src, const ProxOp& op, cudaStream_t s
   if (occ < 1) return set_error(LLR_ERR_UNSUPPORTED, "prox kernel cannot be resident (smem %zu B)", L.total);
   const long long grid = std::min<long long>(src.nblocks, (long long)nsm * occ);
   if (grid < 1) return LLR_OK;
+  note_launch();
   kern<<<(unsigned)grid, kLlrThreads, L.total, stream>>>(src, op, L);
   LLR_CUDA_TRY(cudaGetLastError());
   return LLR_OK;
@@ -919,6 +920,7 @@ int launch_split_instance(const BlockSource& src, const ProxOp& op, cudaStream_t
     LLR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kLlrThreads, L.total));
     if (occ < 1) return set_error(LLR_ERR_UNSUPPORTED, "Gram kernel cannot be resident (smem %zu B)", L.total);
     const long long grid = std::min<long long>(src.nblocks, (long long)nsm * occ);
+    note_launch();
     kern<<<(unsigned)grid, kLlrThreads, L.total, stream>>>(src, op, L);
     LLR_CUDA_TRY(cudaGetLastError());
   }
@@ -930,6 +932,7 @@ int launch_split_instance(const BlockSource& src, const ProxOp& op, cudaStream_t
     LLR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kEigThreads, L.total));
     if (occ < 1) return set_error(LLR_ERR_UNSUPPORTED, "eigen kernel cannot be resident (smem %zu B)", L.total);
     const long long grid = std::min<long long>(src.nblocks, (long long)nsm * occ);
+    note_launch();
     kern<<<(unsigned)grid, kEigThreads, L.total, stream>>>(src, op, L);
     LLR_CUDA_TRY(cudaGetLastError());
   }

@@ -330,6 +330,7 @@ inline unsigned grid_for(long long n, int bs = 256, long long cap = 148LL * 32) 
 int launch_ref_to_planar(const float2* ref, float2* planar, const Geom& g, float scale, PhaseTab ph, int phase_sign,
                          cudaStream_t s) {
   dim3 grid((unsigned)((g.nx + 31) / 32), (unsigned)((g.nyz + 31) / 32), (unsigned)g.nq);
+  note_launch();
   transpose_kernel<<<grid, dim3(32, 8), 0, s>>>(ref, planar, g, 1, scale, ph, phase_sign);
   LLR_CUDA_TRY(cudaGetLastError());
   return LLR_OK;
@@ -338,6 +339,7 @@ int launch_ref_to_planar(const float2* ref, float2* planar, const Geom& g, float
 int launch_planar_to_ref(const float2* planar, float2* ref, const Geom& g, float scale, PhaseTab ph, int phase_sign,
                          cudaStream_t s) {
   dim3 grid((unsigned)((g.nyz + 31) / 32), (unsigned)((g.nx + 31) / 32), (unsigned)g.nq);
+  note_launch();
   transpose_kernel<<<grid, dim3(32, 8), 0, s>>>(planar, ref, g, 0, scale, ph, phase_sign);
   LLR_CUDA_TRY(cudaGetLastError());
   return LLR_OK;
@@ -346,6 +348,7 @@ int launch_planar_to_ref(const float2* planar, float2* ref, const Geom& g, float
 int launch_scale_uncovered(float2* data, const Geom& g, const int* cover, const long long* it_ptr,
                            unsigned long long seed, const int shift[3], const int maxs[3], float scale, PhaseTab ph,
                            int conj_phase, cudaStream_t s) {
+  note_launch();
   uncovered_kernel<<<grid_for(g.V * g.nq), 256, 0, s>>>(data, g, cover[0], cover[1], cover[2], it_ptr, seed,
                                                         shift ? shift[0] : 0, shift ? shift[1] : 0,
                                                         shift ? shift[2] : 0, maxs[0], maxs[1], maxs[2], scale, ph,
@@ -358,6 +361,7 @@ int launch_dc_hybrid(float2* u, const float2* yhat, const int* pos, const long l
                      double* partials, int n_part_x, int replace_only, cudaStream_t s) {
   dim3 grid((unsigned)n_part_x, (unsigned)g.nq);
   (void)max_lines;
+  note_launch();
   dc_hybrid_kernel<<<grid, 256, 0, s>>>(u, yhat, pos, off, g, partials, replace_only);
   LLR_CUDA_TRY(cudaGetLastError());
   return LLR_OK;
@@ -365,6 +369,7 @@ int launch_dc_hybrid(float2* u, const float2* yhat, const int* pos, const long l
 
 int launch_dc_full(float2* u, const float2* yhat, long long n, double* partials, int nblocks, int replace_only,
                    cudaStream_t s) {
+  note_launch();
   dc_full_kernel<<<nblocks, 256, 0, s>>>(u, yhat, n, partials, replace_only);
   LLR_CUDA_TRY(cudaGetLastError());
   return LLR_OK;
@@ -372,6 +377,7 @@ int launch_dc_full(float2* u, const float2* yhat, long long n, double* partials,
 
 int launch_finalize(const double* partials, int np, double scale, double* hist, long long cap, long long* it,
                     int advance, double* out, cudaStream_t s) {
+  note_launch();
   finalize_kernel<<<1, 256, 0, s>>>(partials, np, scale, hist, cap, it, advance, out);
   LLR_CUDA_TRY(cudaGetLastError());
   return LLR_OK;
@@ -379,12 +385,14 @@ int launch_finalize(const double* partials, int np, double scale, double* hist, 
 
 int launch_line_nnz(const float2* y, long long nlines, int nx, int* cnt, cudaStream_t s) {
   long long threads = nlines * 32;
+  note_launch();
   line_nnz_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(y, nlines, nx, cnt);
   LLR_CUDA_TRY(cudaGetLastError());
   return LLR_OK;
 }
 
 int launch_energy(const float2* y, long long n, double* part_e, double* part_n, int nblocks, cudaStream_t s) {
+  note_launch();
   energy_kernel<<<nblocks, 256, 0, s>>>(y, n, part_e, part_n);
   LLR_CUDA_TRY(cudaGetLastError());
   return LLR_OK;
@@ -393,12 +401,14 @@ int launch_energy(const float2* y, long long n, double* part_e, double* part_n, 
 int launch_gather_lines(const float2* yh, float2* yhat, const int* pos, const long long* off, const Geom& g,
                         PhaseTab ph_img, float scale, cudaStream_t s) {
   dim3 grid(256, (unsigned)g.nq);
+  note_launch();
   gather_lines_kernel<<<grid, 256, 0, s>>>(yh, yhat, pos, off, g, ph_img, scale);
   LLR_CUDA_TRY(cudaGetLastError());
   return LLR_OK;
 }
 
 int launch_prep_full(float2* y, const Geom& g, PhaseTab ph_img, float scale, cudaStream_t s) {
+  note_launch();
   prep_full_kernel<<<grid_for(g.V * g.nq), 256, 0, s>>>(y, g, ph_img, scale);
   LLR_CUDA_TRY(cudaGetLastError());
   return LLR_OK;
@@ -406,24 +416,28 @@ int launch_prep_full(float2* y, const Geom& g, PhaseTab ph_img, float scale, cud
 
 int launch_phase_ref(float2* x, const Geom& g, int nvol, const float2* tx, const float2* ty, const float2* tz, int sign,
                      float scale, cudaStream_t s) {
+  note_launch();
   phase_ref_kernel<<<grid_for(g.V * nvol), 256, 0, s>>>(x, g, nvol, tx, ty, tz, sign, scale);
   LLR_CUDA_TRY(cudaGetLastError());
   return LLR_OK;
 }
 
 int launch_phase_x(float2* x, const Geom& g, int nvol, const float2* tx, int sign, float scale, cudaStream_t s) {
+  note_launch();
   phase_x_kernel<<<grid_for(g.V * nvol), 256, 0, s>>>(x, g, nvol, tx, sign, scale);
   LLR_CUDA_TRY(cudaGetLastError());
   return LLR_OK;
 }
 
 int launch_scale(float2* x, long long n, float sc, cudaStream_t s) {
+  note_launch();
   scale_kernel<<<grid_for(n), 256, 0, s>>>(x, n, sc);
   LLR_CUDA_TRY(cudaGetLastError());
   return LLR_OK;
 }
 
 int launch_hard_project(float2* x, const float2* y, long long n, double* partials, int nblocks, cudaStream_t s) {
+  note_launch();
   hard_project_kernel<<<nblocks, 256, 0, s>>>(x, y, n, partials);
   LLR_CUDA_TRY(cudaGetLastError());
   return LLR_OK;

@@ -225,9 +225,12 @@ int wavelet_denoise_strided_xf(const WaveletPlan& p, float2* data, long long sx,
     const int* c = &p.sizes[3 * (l + 1)];
     View T1 = work_view(t1base, 2 * c[0], e[1], e[2]);
     View T2 = work_view(t2base, 2 * c[0], 2 * c[1], e[2]);
+    note_launch();
     analysis_kernel<<<grid_for((long long)T1.sv * nvol), 256, 0, s>>>(in, T1, 0, c[0], td, nvol, 0.f, 0, 0, 0, 0);
+    note_launch();
     analysis_kernel<<<grid_for((long long)T2.sv * nvol), 256, 0, s>>>(T1, T2, 1, c[1], td, nvol, 0.f, 0, 0, 0, 0);
     const int last = (l == L - 1);
+    note_launch();
     analysis_kernel<<<grid_for((long long)D[l].sv * nvol), 256, 0, s>>>(T2, D[l], 2, c[2], td, nvol, alpha, !last,
                                                                          c[0], c[1], c[2]);
     LLR_CUDA_TRY(cudaGetLastError());
@@ -241,15 +244,19 @@ int wavelet_denoise_strided_xf(const WaveletPlan& p, float2* data, long long sx,
     const int* c = &p.sizes[3 * (l + 1)];
     View T1 = work_view(t1base, 2 * c[0], e[1], e[2]);
     View T2 = work_view(t2base, 2 * c[0], 2 * c[1], e[2]);
+    note_launch();
     synthesis_kernel<<<grid_for((long long)T2.sv * nvol), 256, 0, s>>>(D[l], T2, 2, c[2], tr, nvol, none);
+    note_launch();
     synthesis_kernel<<<grid_for((long long)T1.sv * nvol), 256, 0, s>>>(T2, T1, 1, c[1], tr, nvol, none);
     View out;
     if (l > 0) {
       out = D[l - 1];
       out.e[0] = e[0]; out.e[1] = e[1]; out.e[2] = e[2];
+      note_launch();
       synthesis_kernel<<<grid_for((long long)e[0] * e[1] * e[2] * nvol), 256, 0, s>>>(T1, out, 0, c[0], tr, nvol, none);
     } else {
       out = vol;
+      note_launch();
       synthesis_kernel<<<grid_for((long long)e[0] * e[1] * e[2] * nvol), 256, 0, s>>>(T1, out, 0, c[0], tr, nvol, xf);
     }
     LLR_CUDA_TRY(cudaGetLastError());
@@ -352,10 +359,12 @@ int launch_dwt_axis_ref(const float2* vol, float2* dec, const uint32_t* vs, cons
   const int s0 = sh ? sh[0] : 0, s1 = sh ? sh[1] : 0, s2 = sh ? sh[2] : 0;
   if (!inverse) {
     const long long tot = (long long)ds[0] * ds[1] * ds[2];
+    note_launch();
     dwt_axis_ref_kernel<<<grid_for(tot), 256, 0, s>>>(vol, dec, vs[0], vs[1], vs[2], ds[0], ds[1], ds[2], axis, t, s0,
                                                       s1, s2);
   } else {
     const long long tot = (long long)vs[0] * vs[1] * vs[2];
+    note_launch();
     idwt_axis_ref_kernel<<<grid_for(tot), 256, 0, s>>>(const_cast<float2*>(vol), dec, vs[0], vs[1], vs[2], ds[0],
                                                        ds[1], ds[2], axis, t, s0, s1, s2);
   }

@@ -104,6 +104,7 @@ SIGNATURES = {
     "llr_iterate_async": (C.c_int, [P, I32]),
     "llr_iterate_profiled": (C.c_int, [P, I32, PF64, PF64]),
     "llr_iterate_timed": (C.c_int, [P, I32, PF64]),
+    "llr_ctx_kernel_launches": (C.c_int, [P, C.POINTER(I32)]),
     "llr_get_iteration": (C.c_int, [P, C.POINTER(I64)]),
     "llr_set_iteration": (C.c_int, [P, I64]),
     "llr_get_residual_history": (C.c_int, [P, PF64, I32]),

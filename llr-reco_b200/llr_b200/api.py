@@ -206,6 +206,13 @@ class ReconContext:
         return st, tot.value
 
     @property
+    def kernel_launches_per_iteration(self) -> int:
+        """Library kernels (not cuFFT's) one captured iteration launches."""
+        v = C.c_int32()
+        check(lib.llr_ctx_kernel_launches(self.h, C.byref(v)))
+        return int(v.value)
+
+    @property
     def iteration(self) -> int:
         v = C.c_int64()
         check(lib.llr_get_iteration(self.h, C.byref(v)))

@@ -186,6 +186,7 @@ def test_upload_download_round_trip_and_resume(gpu):
         a.upload_kspace(d.y)
         a.init_zero_filled()
         a.iterate(3)
+        assert a.kernel_launches_per_iteration >= 3   # prox, DC, residual finalise at least
         mid = a.download_image()
         a.iterate(2)
         straight = a.download_image()
@@ -205,6 +206,9 @@ def test_state_errors(gpu):
     with ReconContext(p) as ctx:
         with pytest.raises(llr_b200.LlrError) as e:
             ctx.iterate(1)
+        assert e.value.status == L.LLR_ERR_STATE
+        with pytest.raises(llr_b200.LlrError) as e:
+            ctx.kernel_launches_per_iteration
         assert e.value.status == L.LLR_ERR_STATE
         with pytest.raises(llr_b200.LlrError):
             ctx.download_image()
