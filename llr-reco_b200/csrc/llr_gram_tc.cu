@@ -128,13 +128,17 @@ __global__ void __launch_bounds__(kTcThreads, 2) llr_gram_tc_kernel(BlockSource 
   bool used[2] = {false, false};
   bool failed = false;
 
-  for (long long blk = blockIdx.x; blk < src.nblocks && !failed; blk += gridDim.x) {
-    const long long base = src.kind == 1 ? 0 : blk * (long long)m * n;
+  // Lane layout of the gather: 8 volumes x 4 consecutive rows per warp instruction, so one
+  // request covers 8 short runs of the planar layout; warp w owns volume groups 2w and 2w+1.
+  // In shared memory the same lanes write 32 consecutive words of one core-matrix row block.
+  const int qsub = lane >> 2, usub = lane & 3;
+  float2 pre[2][kKB];
+  auto build_rows = [&](long long b) {
     for (int r = tid; r < m; r += kTcThreads) {
       TcRowTab rt;
       if (src.kind == 1) {
         int ix, iy, iz;
-        block_row_coord(src, blk, sh, r, ix, iy, iz);
+        block_row_coord(src, b, sh, r, ix, iy, iz);
         rt.off = (int)planar_index(src.g, ix, iy, iz, 0);
         rt.cx = ix;
         rt.cyz = iy | (iz << 16);
@@ -147,29 +151,38 @@ __global__ void __launch_bounds__(kTcThreads, 2) llr_gram_tc_kernel(BlockSource 
       rt.pad = 0;
       rows[r] = rt;
     }
-    // operand planes start zeroed (rows 2n..127 and K padding must contribute nothing)
-    for (int i = tid; i < 4 * kOpBytes / 16; i += kTcThreads)
-      reinterpret_cast<float4*>(ops)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-    __syncthreads();
+  };
+  auto load_chunk = [&](int c, long long base) {
+    const int c0 = c * kKC;
+    int roff[kKB];
+#pragma unroll
+    for (int kb = 0; kb < kKB; ++kb) {
+      const int r = c0 + 4 * kb + usub;
+      roff[kb] = r < m ? rows[r].off : -1;
+    }
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      const int q = 8 * (2 * warp + t) + qsub;
+      const float2* col = src.data + base + (long long)q * qstride;
+#pragma unroll
+      for (int kb = 0; kb < kKB; ++kb)
+        pre[t][kb] = (q < n && roff[kb] >= 0) ? col[roff[kb]] : make_float2(0.f, 0.f);
+    }
+  };
+  auto block_base = [&](long long b) { return src.kind == 1 ? 0ll : b * (long long)m * n; };
 
-    // Register prefetch: each thread owns up to kTasks (kb, q) tasks of a chunk, 4 rows each.
-    constexpr int kTasks = 4;
-    float2 pre[kTasks][4];
-    auto load_chunk = [&](int c) {
-      const int c0 = c * kKC;
-#pragma unroll
-      for (int t = 0; t < kTasks; ++t) {
-        const int task = tid + t * kTcThreads;
-        const int kb = task / n, q = task - kb * n;
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int r = c0 + 4 * kb + u;
-          pre[t][u] = make_float2(0.f, 0.f);
-          if (task < kKB * n && r < m) pre[t][u] = src.data[base + (long long)rows[r].off + (long long)q * qstride];
-        }
-      }
-    };
-    load_chunk(0);
+  // operand planes start zeroed: rows 2n..127 (M padding) are never written by the gather
+  for (int i = tid; i < 4 * kOpBytes / 16; i += kTcThreads)
+    reinterpret_cast<float4*>(ops)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+  long long blk = blockIdx.x;
+  if (blk < src.nblocks) {
+    build_rows(blk);
+    __syncthreads();
+    load_chunk(0, block_base(blk));
+  }
+
+  for (; blk < src.nblocks && !failed; blk += gridDim.x) {
+    const long long nxt = blk + gridDim.x;
     for (int c = 0; c < nchunks; ++c) {
       const int b = c & 1;
       if (used[b]) {  // the MMAs that read this buffer two chunks ago must be done
@@ -181,16 +194,13 @@ __global__ void __launch_bounds__(kTcThreads, 2) llr_gram_tc_kernel(BlockSource 
       unsigned char* lo = hi + kOpBytes;
       const int c0 = c * kKC;
 #pragma unroll
-      for (int t = 0; t < kTasks; ++t) {
-        const int task = tid + t * kTcThreads;
-        if (task >= kKB * n) continue;
-        const int kb = task / n, q = task - kb * n;
-        uint4 rh, ih, rl, il;
-        uint32_t* prh = &rh.x; uint32_t* pih = &ih.x; uint32_t* prl = &rl.x; uint32_t* pil = &il.x;
+      for (int t = 0; t < 2; ++t) {
+        const int q = 8 * (2 * warp + t) + qsub;
+        if (q >= n) continue;
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int r = c0 + 4 * kb + u;
-          float2 x = pre[t][u];
+        for (int kb = 0; kb < kKB; ++kb) {
+          const int r = c0 + 4 * kb + usub;
+          float2 x = pre[t][kb];
           if (src.kind == 1 && r < m) {
             float2 p;
             if (src.ph_uniform) p = rowph[r];
@@ -201,17 +211,14 @@ __global__ void __launch_bounds__(kTcThreads, 2) llr_gram_tc_kernel(BlockSource 
             x = cscale(cmul_bc(x, p), src.load_scale);
           }
           const uint32_t a = tf32_rna(x.x), bb = tf32_rna(x.y);
-          prh[u] = a;
-          pih[u] = bb;
-          prl[u] = __float_as_uint(x.x - __uint_as_float(a));
-          pil[u] = __float_as_uint(x.y - __uint_as_float(bb));
+          const int oq = op_offset(q, kb) + 4 * usub, oi = op_offset(n + q, kb) + 4 * usub;
+          *reinterpret_cast<uint32_t*>(hi + oq) = a;
+          *reinterpret_cast<uint32_t*>(hi + oi) = bb;
+          *reinterpret_cast<uint32_t*>(lo + oq) = __float_as_uint(x.x - __uint_as_float(a));
+          *reinterpret_cast<uint32_t*>(lo + oi) = __float_as_uint(x.y - __uint_as_float(bb));
         }
-        *reinterpret_cast<uint4*>(hi + op_offset(q, kb)) = rh;
-        *reinterpret_cast<uint4*>(hi + op_offset(n + q, kb)) = ih;
-        *reinterpret_cast<uint4*>(lo + op_offset(q, kb)) = rl;
-        *reinterpret_cast<uint4*>(lo + op_offset(n + q, kb)) = il;
       }
-      if (c + 1 < nchunks) load_chunk(c + 1);   // in flight while the tensor core works
+      if (c + 1 < nchunks) load_chunk(c + 1, block_base(blk));   // in flight while the tensor core works
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncthreads();
       if (tid == 0) {
@@ -231,6 +238,13 @@ __global__ void __launch_bounds__(kTcThreads, 2) llr_gram_tc_kernel(BlockSource 
       used[b] = true;
     }
     if (failed) break;
+    // the row table is free once the last chunk is converted: the next block's table and its
+    // first chunk's loads go out now and overlap the MMAs' tail and this block's epilogue
+    if (nxt < src.nblocks) {
+      build_rows(nxt);
+      __syncthreads();
+      load_chunk(0, block_base(nxt));
+    }
     // all MMAs of this block complete -> read P and stage it in the (now idle) operand area
     {
       const bool ok = mbar_wait(smem_u32(&hdr->mbar[2]), phase[2]);
@@ -275,6 +289,13 @@ __global__ void __launch_bounds__(kTcThreads, 2) llr_gram_tc_kernel(BlockSource 
       const float re = Ps[ii * ldp + j] + Ps[(n + ii) * ldp + n + j];
       const float im = Ps[ii * ldp + n + j] - Ps[(n + ii) * ldp + j];
       G[idx] = make_float2(re, im);
+    }
+    __syncthreads();
+    // the staging overwrote the padding rows 2n..127 of the operand planes: zero them again
+    for (int i = tid; i < 4 * (128 - 2 * n) * kKB; i += kTcThreads) {
+      const int plane = i / ((128 - 2 * n) * kKB), rem = i - plane * ((128 - 2 * n) * kKB);
+      const int mn = 2 * n + rem / kKB, kb = rem - (rem / kKB) * kKB;
+      *reinterpret_cast<float4*>(ops + (size_t)plane * kOpBytes + op_offset(mn, kb)) = make_float4(0.f, 0.f, 0.f, 0.f);
     }
     __syncthreads();
   }
