@@ -66,7 +66,8 @@ typedef struct llr_config {
   int32_t n_iter;             /* default iteration count (lib.rs:62)                 */
   uint64_t seed;              /* key of the counter-based shift RNG                  */
   int32_t device;             /* CUDA device ordinal                                 */
-  int32_t eig_solver;         /* 0: tridiagonal + bisection (default); 1: Jacobi      */
+  int32_t eig_solver;         /* 0: tridiagonal, warp per block (default); 1: Jacobi;
+                                  2: tridiagonal, CTA per block                          */
   int32_t gram_mode;          /* 0: 3xTF32 tensor cores (default); 1: FP32 FMA        */
   int32_t reserved[5];
 } llr_config;

@@ -198,6 +198,8 @@ static int prox_pass(llr_ctx* c, cudaStream_t s, const int* explicit_shift, bool
     op.fb_list = c->d_fb;
     op.fb_count = c->d_fb + std::max<long long>(1, c->nblocks);
     op.gram = c->d_gram;
+    op.gram_stride = prox_gram_stride(c->g.nq);
+    op.blk_ra = c->d_blk_ra;
     op.gram_mode = c->cfg.gram_mode;
     op.err = c->d_err;
     LLR_TRY(launch_llr_prox(src, op, s));
@@ -301,7 +303,8 @@ int llr_ctx_create(const llr_config* cfg, llr_ctx** out) {
   e = cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream);
   if (e != cudaSuccess) return fail(cuda_error(e, "cudaMemsetAsync", __FILE__, __LINE__));
   if (cfg->subspace_rank == 0 &&
-      (st = dalloc(&c->d_gram, (size_t)std::max<long long>(1, c->nblocks) * ((size_t)c->g.nq * (c->g.nq + 1) / 2))))
+      ((st = dalloc(&c->d_gram, (size_t)std::max<long long>(1, c->nblocks) * (size_t)prox_gram_stride(c->g.nq))) ||
+       (st = dalloc(&c->d_blk_ra, (size_t)std::max<long long>(1, c->nblocks) + 1))))
     return fail(st);
   e = cudaMemsetAsync(c->d_iter, 0, sizeof(long long), c->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(c->d_hist, 0, sizeof(double) * c->hist_cap, c->stream);
@@ -336,7 +339,7 @@ int llr_ctx_destroy(llr_ctx* c) {
   if (c->have_plan) cufftDestroy(c->plan_fwd);
   dfree(c->d_x); dfree(c->d_work); dfree(c->d_yhat); dfree(c->d_samp_pos); dfree(c->d_samp_off);
   dfree(c->d_ph_ksp); dfree(c->d_ph_img); dfree(c->d_S); dfree(c->d_partials); dfree(c->d_hist); dfree(c->d_iter);
-  dfree(c->d_block_stat); dfree(c->d_fb); dfree(c->d_gram); dfree(c->d_err); dfree(c->d_wavelet_work); dfree(c->d_fft_work);
+  dfree(c->d_block_stat); dfree(c->d_fb); dfree(c->d_gram); dfree(c->d_blk_ra); dfree(c->d_err); dfree(c->d_wavelet_work); dfree(c->d_fft_work);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return LLR_OK;
@@ -837,6 +840,7 @@ int llr_ctx_device_bytes(const llr_ctx* c, size_t* bytes) {
   size_t b = 2 * E * sizeof(float2);
   b += c->hybrid ? (size_t)c->n_samp_lines * c->g.nx * sizeof(float2) : (c->have_kspace ? E * sizeof(float2) : 0);
   b += c->fft_work_bytes + c->wavelet_work_elems * sizeof(float2);
+  if (c->d_gram) b += (size_t)std::max<long long>(1, c->nblocks) * (size_t)prox_gram_stride(c->g.nq) * sizeof(float2);
   *bytes = b;
   return LLR_OK;
 }

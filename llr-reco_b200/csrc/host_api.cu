@@ -188,7 +188,7 @@ int llr_config_validate(const llr_config* c) {
   if (c->subspace_rank > 0 && c->prox_mode == LLR_PROX_HARD_RANK && c->rank > c->subspace_rank)
     return set_error(LLR_ERR_INVALID, "llr rank must be <= subspace rank (lib.rs:217)");
   if (!(c->wavelet_alpha >= 0.f)) return set_error(LLR_ERR_INVALID, "wavelet_alpha must be >= 0");
-  if (c->eig_solver != 0 && c->eig_solver != 1) return set_error(LLR_ERR_INVALID, "eig_solver must be 0 or 1");
+  if (c->eig_solver < 0 || c->eig_solver > 2) return set_error(LLR_ERR_INVALID, "eig_solver must be 0, 1 or 2");
   if (c->gram_mode != 0 && c->gram_mode != 1) return set_error(LLR_ERR_INVALID, "gram_mode must be 0 or 1");
   if (c->wavelet_alpha > 0.f && (c->wavelet_moments < 1 || c->wavelet_moments > 10))
     return set_error(LLR_ERR_INVALID, "wavelet_moments must be in [1, 10]");
@@ -358,15 +358,18 @@ static int batch_prox(int m, int n, int mode, int rank, float lam, int batch, ll
   op.eig_solver = g_batch_eig_solver;
   int* fb = nullptr;
   float2* gram = nullptr;
-  LLR_CUDA_TRY(cudaMallocAsync((void**)&fb, sizeof(int) * ((size_t)batch + 1), s));
-  cudaError_t e = cudaMallocAsync((void**)&gram, sizeof(float2) * (size_t)batch * ((size_t)n * (n + 1) / 2), s);
+  // fallback list + count, then the per-block kept counts + queue counter
+  LLR_CUDA_TRY(cudaMallocAsync((void**)&fb, sizeof(int) * (2 * (size_t)batch + 2), s));
+  cudaError_t e = cudaMallocAsync((void**)&gram, sizeof(float2) * (size_t)batch * (size_t)prox_gram_stride(n), s);
   if (e != cudaSuccess) {
     cudaFreeAsync(fb, s);
     return cuda_error(e, "cudaMallocAsync", __FILE__, __LINE__);
   }
   op.fb_list = fb;
   op.fb_count = fb + batch;
+  op.blk_ra = fb + batch + 1;
   op.gram = gram;
+  op.gram_stride = prox_gram_stride(n);
   op.gram_mode = 0;
   op.err = nullptr;
   int st = launch_llr_prox(src, op, s);

@@ -281,7 +281,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) llr_gram_tc_kernel(BlockSource 
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
-    float2* G = op.gram + blk * Pn;
+    float2* G = op.gram + blk * op.gram_stride;
     for (long long idx = tid; idx < Pn; idx += kTcThreads) {
       const int i = (int)((sqrtf(8.f * (float)idx + 1.f) - 1.f) * 0.5f);
       const int ii = ((long long)i * (i + 1) / 2 > idx) ? i - 1 : (((long long)(i + 1) * (i + 2) / 2 <= idx) ? i + 1 : i);

@@ -39,13 +39,27 @@ struct ProxOp {
   int rank;
   float lambda;
   float* block_stat;   // when non-null: write the largest Gram eigenvalue, skip the update
-  int eig_solver;      // 0: tridiagonal + bisection + inverse iteration; 1: Jacobi
+  int eig_solver;      // 0: tridiagonal, one warp per block; 1: Jacobi; 2: tridiagonal, one CTA per block
   int* fb_list;        // blocks handed to the Jacobi kernel (capacity nblocks)
   int* fb_count;
-  float2* gram;        // optional scratch, nblocks * n(n+1)/2: selects the split Gram/eigen path
+  float2* gram;        // optional scratch, nblocks * gram_stride: selects the split Gram/eigen path
+  long long gram_stride;   // float2 per block in `gram` (prox_gram_stride(n))
+  int* blk_ra;         // split path: kept count per block (+1 int: the eigen kernel's queue)
   int gram_mode;       // 0: 3xTF32 on tensor cores (tcgen05) where 2n <= 128; 1: FP32 FMA
   int* err;            // device flag set when a bounded wait gives up (never expected)
 };
+
+// Kept eigenvectors per block that the warp eigen kernel hands to the apply kernel.
+constexpr int kFacCols = 8;
+
+// Per-block scratch of the split prox path, in float2: the packed Gram matrix n(n+1)/2,
+// overwritten by the eigen factor (n x kFacCols eigenvectors, then kFacCols gains).
+inline long long prox_gram_stride(int n) {
+  const long long p = (long long)n * (n + 1) / 2, f = (long long)n * kFacCols + kFacCols;
+  return p > f ? p : f;
+}
+
+int launch_llr_eig_warp(const ProxOp& op, long long nblocks, cudaStream_t stream);
 
 int launch_llr_prox(const BlockSource& src, const ProxOp& op, cudaStream_t stream);
 bool llr_prox_supported(int m, int n);
@@ -126,6 +140,7 @@ struct llr_ctx {
   float* d_block_stat;
   int* d_fb;                // Jacobi fallback block list (nblocks) + count
   float2* d_gram;           // per-block packed Gram matrices (split prox path)
+  int* d_blk_ra;            // per-block kept count of the split prox path + queue counter
   int* d_err;               // device error flag of the prox kernels
   int ph_uniform;           // all volumes share the image-domain phase tables
   float2* d_wavelet_work;

@@ -486,7 +486,7 @@ TrdLayout make_trd_layout(int m, int n) {
   return L;
 }
 
-template <int RM>
+template <int RM, int LDV = kRaMax>
 __device__ void apply_rows(const BlockSource& s, long long base, const RowTab* rows, const float2* rowph, int m, int n,
                            long long qstride, const float2* Va, const float* g, int ra) {
   constexpr int KB = 8;   // loads in flight per thread
@@ -505,7 +505,7 @@ __device__ void apply_rows(const BlockSource& s, long long base, const RowTab* r
         if (k0 + u < n) {
 #pragma unroll
           for (int a = 0; a < RM; ++a)
-            if (a < ra) cfma(t[a], c[u], Va[(k0 + u) * kRaMax + a]);
+            if (a < ra) cfma(t[a], c[u], Va[(k0 + u) * LDV + a]);
         }
       }
     }
@@ -516,7 +516,7 @@ __device__ void apply_rows(const BlockSource& s, long long base, const RowTab* r
       float2 c = make_float2(0.f, 0.f);
 #pragma unroll
       for (int a = 0; a < RM; ++a)
-        if (a < ra) cfma_cb(c, t[a], Va[q * kRaMax + a]);
+        if (a < ra) cfma_cb(c, t[a], Va[q * LDV + a]);
       store_elem(s, base, rt, rowph, r, q, qstride, c);
     }
   }
@@ -762,13 +762,12 @@ __global__ void __launch_bounds__(kLlrThreads, 2) llr_gram_kernel(BlockSource sr
   float2* Cch = reinterpret_cast<float2*>(smem + L.off_C);
   const int m = op.m, n = op.n;
   const long long qstride = src.kind == 1 ? src.g.V : (long long)m;
-  const long long P = (long long)n * (n + 1) / 2;
   if (threadIdx.x == 0) block_shift(src, misc->shift);
   __syncthreads();
   const int sh[3] = {misc->shift[0], misc->shift[1], misc->shift[2]};
   for (long long blk = blockIdx.x; blk < src.nblocks; blk += gridDim.x) {
     const long long base = src.kind == 1 ? 0 : blk * (long long)m * n;
-    float2* G = op.gram + blk * P;
+    float2* G = op.gram + blk * op.gram_stride;
     gram_block<NPMAX, TG>(src, L, m, n, blk, base, qstride, sh, rows, rowph, Cch, [&](int i, int j, float2 v) {
       if (j <= i) G[(i * (i + 1)) / 2 + j] = v;
     });
@@ -816,7 +815,7 @@ __global__ void __launch_bounds__(kEigThreads, 4) llr_eig_apply_kernel(BlockSour
 
   for (long long blk = blockIdx.x; blk < src.nblocks; blk += gridDim.x) {
     const long long base = src.kind == 1 ? 0 : blk * (long long)m * n;
-    const float2* G = op.gram + blk * (long long)P;
+    const float2* G = op.gram + blk * op.gram_stride;
     float fro = 0.f;   // ||G||_F^2 from the packed lower triangle
     for (int i = tid; i < P; i += blockDim.x) {
       const float2 v = G[i];
@@ -905,6 +904,95 @@ __global__ void __launch_bounds__(kEigThreads, 4) llr_eig_apply_kernel(BlockSour
   }
 }
 
+// C' = (C V_a) diag(g) V_a^H for the blocks whose eigen factor the warp eigen kernel wrote
+// (r_a > 0), zero for r_a = 0; r_a = -1 (Jacobi fallback) and -2 (identity) are left alone.
+// One CTA per block, one thread per row with eight loads in flight.
+constexpr int kApplyThreads = 256;
+
+struct ApplyLayout {
+  size_t off_row, off_rowph, off_V, off_g, total;
+};
+
+inline ApplyLayout make_apply_layout(int m, int n) {
+  ApplyLayout L;
+  size_t off = 64;
+  L.off_row = off; off = align16(off + sizeof(RowTab) * (size_t)m);
+  L.off_rowph = off; off = align16(off + sizeof(float2) * (size_t)m);
+  L.off_V = off; off = align16(off + sizeof(float2) * (size_t)n * kFacCols);
+  L.off_g = off; off = align16(off + sizeof(float) * kFacCols);
+  L.total = off;
+  return L;
+}
+
+__global__ void __launch_bounds__(kApplyThreads, 4) llr_apply_kernel(BlockSource src, ProxOp op, ApplyLayout L) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  int* sh_s = reinterpret_cast<int*>(smem);
+  RowTab* rows = reinterpret_cast<RowTab*>(smem + L.off_row);
+  float2* rowph = reinterpret_cast<float2*>(smem + L.off_rowph);
+  float2* Va = reinterpret_cast<float2*>(smem + L.off_V);
+  float* g = reinterpret_cast<float*>(smem + L.off_g);
+  const int m = op.m, n = op.n, tid = threadIdx.x;
+  const long long qstride = src.kind == 1 ? src.g.V : (long long)m;
+  if (tid == 0) block_shift(src, sh_s);
+  __syncthreads();
+  const int sh[3] = {sh_s[0], sh_s[1], sh_s[2]};
+  for (long long blk = blockIdx.x; blk < src.nblocks; blk += gridDim.x) {
+    const int ra = op.blk_ra[blk];
+    if (ra < 0) continue;   // uniform over the CTA
+    const long long base = src.kind == 1 ? 0 : blk * (long long)m * n;
+    for (int r = tid; r < m; r += blockDim.x) {
+      RowTab rt;
+      if (src.kind == 1) {
+        int ix, iy, iz;
+        block_row_coord(src, blk, sh, r, ix, iy, iz);
+        rt.off = (int)planar_index(src.g, ix, iy, iz, 0);
+        rt.cx = ix;
+        rt.cyz = iy | (iz << 16);
+        if (src.ph_uniform) rowph[r] = phase_at(src.ph, src.g, 0, ix, iy, iz);
+      } else {
+        rt.off = r;
+        rt.cx = 0;
+        rt.cyz = 0;
+      }
+      rt.pad = 0;
+      rows[r] = rt;
+    }
+    if (ra > 0) {
+      const float2* F = op.gram + blk * op.gram_stride;
+      for (int i = tid; i < n * kFacCols; i += blockDim.x) Va[i] = F[i];
+      if (tid < kFacCols) g[tid] = F[n * kFacCols + tid].x;
+    }
+    __syncthreads();
+    if (ra == 0) {
+      for (int idx = tid; idx < m * n; idx += blockDim.x) {
+        const int q = idx / m, r = idx - q * m;
+        store_elem(src, base, rows[r], rowph, r, q, qstride, make_float2(0.f, 0.f));
+      }
+    } else if (ra <= 2) {
+      apply_rows<2, kFacCols>(src, base, rows, rowph, m, n, qstride, Va, g, ra);
+    } else if (ra <= 4) {
+      apply_rows<4, kFacCols>(src, base, rows, rowph, m, n, qstride, Va, g, ra);
+    } else {
+      apply_rows<kFacCols, kFacCols>(src, base, rows, rowph, m, n, qstride, Va, g, ra);
+    }
+    __syncthreads();
+  }
+}
+
+int launch_apply(const BlockSource& src, const ProxOp& op, cudaStream_t stream) {
+  const ApplyLayout L = make_apply_layout(op.m, op.n);
+  if (L.total > 227 * 1024) return set_error(LLR_ERR_UNSUPPORTED, "apply kernel needs %zu B smem", L.total);
+  LLR_CUDA_TRY(cudaFuncSetAttribute(llr_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total));
+  // room for eight resident CTAs (the thread limit); the rest of the SM's memory stays L1
+  const int carve = (int)std::min<size_t>(100, (8 * (L.total + 1024) * 100) / (228 * 1024) + 1);
+  LLR_CUDA_TRY(cudaFuncSetAttribute(llr_apply_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
+  const long long grid = std::min<long long>(src.nblocks, 1ll << 30);
+  note_launch();
+  llr_apply_kernel<<<(unsigned)grid, kApplyThreads, L.total, stream>>>(src, op, L);
+  LLR_CUDA_TRY(cudaGetLastError());
+  return LLR_OK;
+}
+
 template <int NPMAX, int TG>
 int launch_split_instance(const BlockSource& src, const ProxOp& op, cudaStream_t stream) {
   int dev = 0, nsm = 0, occ = 0;
@@ -923,6 +1011,10 @@ int launch_split_instance(const BlockSource& src, const ProxOp& op, cudaStream_t
     note_launch();
     kern<<<(unsigned)grid, kLlrThreads, L.total, stream>>>(src, op, L);
     LLR_CUDA_TRY(cudaGetLastError());
+  }
+  if (!op.block_stat && op.eig_solver == 0 && op.blk_ra) {   // warp eigen kernel + apply kernel
+    LLR_TRY(launch_llr_eig_warp(op, src.nblocks, stream));
+    return launch_apply(src, op, stream);
   }
   {
     EigLayout L = make_eig_layout<NPMAX>(op.m);

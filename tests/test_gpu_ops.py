@@ -92,6 +92,45 @@ def test_soft_threshold_batch_matches_oracle(gpu, m, n):
     assert rel_err(got, exp) < 5e-5
 
 
+def _spectrum_blocks(rng, m, n, sigmas):
+    """Blocks C = U diag(sigma) V^H with Haar-like random U (m x n) and V (n x n)."""
+    out = np.empty((m, n, len(sigmas)), dtype=np.complex128)
+    for b, sg in enumerate(sigmas):
+        U, _ = np.linalg.qr(crandn(rng, (m, n)))
+        V, _ = np.linalg.qr(crandn(rng, (n, n)))
+        out[:, :, b] = (U * np.asarray(sg)[None, :]) @ V.conj().T
+    return out
+
+
+@pytest.mark.parametrize("n", [61, 17])
+def test_soft_threshold_eigen_branches(gpu, n):
+    """Every branch of the eigen stage: all singular values below the threshold with
+    ||G||_F <= lambda^2 (zero at once) and with ||G||_F above it (zero certified by a
+    Cholesky factorisation of lambda^2 I - G), 1..8 kept components, more than 8 kept
+    (Jacobi fallback), a singular value just above the threshold, and an all-zero block."""
+    rng = np.random.default_rng(21)
+    m, lam = 216, 1.0
+    low = lambda k: list(rng.uniform(0.05, 0.95, k))
+    sig = []
+    sig.append([0.01] * n)                                   # ||G||_F tiny
+    sig.append(low(n))                                       # below, Frobenius above lambda^2
+    sig.append([0.97] * 3 + low(n - 3))                      # close below
+    for r in range(1, 9):
+        sig.append(list(np.linspace(4.0, 1.2, r)) + low(n - r))
+    sig.append(list(np.linspace(5.0, 1.5, 12)) + low(n - 12))  # 12 kept: fallback
+    sig.append([1.0 + 1e-4] + low(n - 1))                    # just above the threshold
+    sig.append([0.0] * n)                                    # all zero
+    A = _spectrum_blocks(rng, m, n, sig).astype(np.complex64)
+    d = DeviceBuffer.from_array(A)
+    L.check(L.lib.llr_soft_threshold_batch_dev(m, n, lam, A.shape[2], d.ptr, None))
+    got = d.download(np.empty_like(A, order="F"))
+    exp = O.low_rank_soft(A.astype(np.complex128), lam)
+    for b in range(A.shape[2]):
+        scale = max(np.linalg.norm(A[:, :, b]), 1e-30)
+        assert np.linalg.norm(got[:, :, b] - exp[:, :, b]) / scale < 5e-5, b
+    assert rel_err(got, exp) < 5e-5
+
+
 def test_zero_and_rank_deficient_blocks(gpu):
     m, n, batch = 64, 8, 3
     A = np.zeros((m, n, batch), dtype=np.complex64)

@@ -80,7 +80,7 @@ def test_soft_threshold_hybrid_path(gpu):
     assert gh[-1] < gh[0]
 
 
-@pytest.mark.parametrize("eig_solver", [0, 1])
+@pytest.mark.parametrize("eig_solver", [0, 1, 2])
 def test_hard_rank_c1_like(gpu, eig_solver):
     """Config-1 shape class: 8^3 blocks, 17 volumes (Casorati 512 x 17), reduced volume."""
     d = dataset((32, 32, 32), 17, accel=4.0, centre=8)
@@ -88,7 +88,7 @@ def test_hard_rank_c1_like(gpu, eig_solver):
     check(gx, ox, gh, oh)
 
 
-@pytest.mark.parametrize("eig_solver,gram_mode", [(0, 0), (1, 0), (0, 1)])
+@pytest.mark.parametrize("eig_solver,gram_mode", [(0, 0), (1, 0), (0, 1), (2, 0)])
 def test_soft_c2_like(gpu, eig_solver, gram_mode):
     """Config-2 shape class: 6^3 blocks, 61 volumes (Casorati 216 x 61), reduced volume; both
     eigen-solvers (tridiagonal + bisection, Jacobi) and both Gram paths (3xTF32 tensor cores,
