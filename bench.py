@@ -195,7 +195,7 @@ def run_b200(args, dist: Dist) -> None:
     E = nx * ny * nz * nq
     params = ReconParams(vol_size=(nx, ny, nz), nq=nq, block_size=c["block"], prox_mode=llr_b200.LLR_PROX_SOFT_THRESH,
                          lam=0.0, seed=args.seed, device=dev, gram_mode=args.gram_mode,
-                         eig_solver=args.eig_solver)
+                         eig_solver=args.eig_solver, fft_mode=args.fft_mode)
     ctx = ReconContext(params)
     ctx.upload_kspace(d.y)
     ctx.init_zero_filled()
@@ -349,6 +349,8 @@ def main(argv=None):
     ap.add_argument("--cpu-blocks", type=int, default=2048)
     ap.add_argument("--cpu-vols", type=int, default=8)
     ap.add_argument("--gram-mode", type=int, default=0, help="0: 3xTF32 tensor-core Gram, 1: FP32 FMA Gram")
+    ap.add_argument("--fft-mode", type=int, default=0,
+                    help="0: fused per-plane FFT + DC + inverse FFT kernel; 1: cuFFT passes")
     ap.add_argument("--eig-solver", type=int, default=0,
                     help="0: tridiagonal, warp per block; 1: Jacobi; 2: tridiagonal, CTA per block")
     args = ap.parse_args(argv)

@@ -69,7 +69,9 @@ typedef struct llr_config {
   int32_t eig_solver;         /* 0: tridiagonal, warp per block (default); 1: Jacobi;
                                   2: tridiagonal, CTA per block                          */
   int32_t gram_mode;          /* 0: 3xTF32 tensor cores (default); 1: FP32 FMA        */
-  int32_t reserved[5];
+  int32_t fft_mode;           /* 0: fused FFT + DC + inverse FFT per (x, volume) plane
+                                  where the plane fits (default); 1: cuFFT passes       */
+  int32_t reserved[4];
 } llr_config;
 
 /* ---- library / errors ------------------------------------------------------------ */

@@ -237,9 +237,18 @@ static int dc_pass(llr_ctx* c, cudaStream_t s, int replace_only) {
 
 static int n_partials(const llr_ctx* c) { return c->hybrid ? kPartX * c->g.nq : kPartFull; }
 
+// Forward 2-D DFT, DC with residual, inverse 2-D DFT in one kernel; residual finalized.
+static int fused_dc_pass(llr_ctx* c, cudaStream_t s, double* out) {
+  LLR_TRY(launch_fft_dc(c->d_x, c->d_yhat, c->d_samp_pos, c->d_samp_off, c->d_fft_tw, c->g, c->d_partials,
+                        c->fft_grid, s));
+  return launch_finalize(c->d_partials, c->fft_grid, (double)c->load_scale, out ? nullptr : c->d_hist,
+                         out ? 0 : c->hist_cap, out ? nullptr : c->d_iter, out ? 0 : 1, out, s);
+}
+
 int ctx_enqueue_iteration(llr_ctx* c, cudaStream_t s) {
   LLR_TRY(prox_pass(c, s, nullptr, false, nullptr));
   if (c->wavelet_on) LLR_TRY(wavelet_pass(c, s, 1.f));
+  if (c->fused_fft) return fused_dc_pass(c, s, nullptr);
   LLR_TRY(exec_fft(c, c->d_x, CUFFT_FORWARD, s));
   LLR_TRY(dc_pass(c, s, 0));
   LLR_TRY(launch_finalize(c->d_partials, n_partials(c), (double)c->load_scale, c->d_hist, c->hist_cap, c->d_iter, 1,
@@ -311,6 +320,15 @@ int llr_ctx_create(const llr_config* cfg, llr_ctx** out) {
   if (e == cudaSuccess) e = cudaMemsetAsync(c->d_x, 0, sizeof(float2) * E, c->stream);
   if (e != cudaSuccess) return fail(cuda_error(e, "cudaMemsetAsync", __FILE__, __LINE__));
   if (cfg->subspace_rank > 0 && (st = dalloc(&c->d_S, (size_t)c->g.nq * cfg->subspace_rank))) return fail(st);
+  if (cfg->fft_mode == 0 && fft_dc_supported(c->g.ny, c->g.nz)) {   // fused FFT + DC twiddles (FP64-computed)
+    const std::vector<float2> tw = fft_dc_twiddles(c->g.ny, c->g.nz);
+    c->fft_grid = fft_dc_grid(c->g.ny, c->g.nz);
+    if (c->fft_grid > 0) {
+      if ((st = dalloc(&c->d_fft_tw, tw.size()))) return fail(st);
+      e = cudaMemcpy(c->d_fft_tw, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) return fail(cuda_error(e, "cudaMemcpy", __FILE__, __LINE__));
+    }
+  }
   c->wavelet_on = false;
   if (cfg->wavelet_alpha > 0.f) {
     if ((st = wavelet_plan_init(&c->wplan, c->g.nx, c->g.ny, c->g.nz, cfg->wavelet_moments, cfg->wavelet_levels)))
@@ -339,7 +357,7 @@ int llr_ctx_destroy(llr_ctx* c) {
   if (c->have_plan) cufftDestroy(c->plan_fwd);
   dfree(c->d_x); dfree(c->d_work); dfree(c->d_yhat); dfree(c->d_samp_pos); dfree(c->d_samp_off);
   dfree(c->d_ph_ksp); dfree(c->d_ph_img); dfree(c->d_S); dfree(c->d_partials); dfree(c->d_hist); dfree(c->d_iter);
-  dfree(c->d_block_stat); dfree(c->d_fb); dfree(c->d_gram); dfree(c->d_blk_ra); dfree(c->d_err); dfree(c->d_wavelet_work); dfree(c->d_fft_work);
+  dfree(c->d_block_stat); dfree(c->d_fb); dfree(c->d_gram); dfree(c->d_blk_ra); dfree(c->d_fft_tw); dfree(c->d_err); dfree(c->d_wavelet_work); dfree(c->d_fft_work);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return LLR_OK;
@@ -411,6 +429,7 @@ static int upload_kspace_device(llr_ctx* c) {
   dfree(c->d_samp_pos); c->d_samp_pos = nullptr;
   dfree(c->d_samp_off); c->d_samp_off = nullptr;
   c->hybrid = structured;
+  c->fused_fft = structured && c->cfg.fft_mode == 0 && c->d_fft_tw != nullptr;
   PhaseTab ph_img_full = ctx_phase(c, c->d_ph_img, true);
   if (structured) {
     // sampled (ky + ny*kz) per volume
@@ -582,14 +601,15 @@ static int capture_stage(llr_ctx* c, int stage, cudaGraphExec_t* out) {
   switch (stage) {
     case 0: st = prox_pass(c, s, nullptr, false, nullptr); break;
     case 1: if (c->wavelet_on) st = wavelet_pass(c, s, 1.f); break;
-    case 2: st = exec_fft(c, c->d_x, CUFFT_FORWARD, s); break;
+    case 2: st = c->fused_fft ? fused_dc_pass(c, s, nullptr) : exec_fft(c, c->d_x, CUFFT_FORWARD, s); break;
     case 3:
+      if (c->fused_fft) break;
       st = dc_pass(c, s, 0);
       if (st == LLR_OK)
         st = launch_finalize(c->d_partials, n_partials(c), (double)c->load_scale, c->d_hist, c->hist_cap, c->d_iter,
                              1, nullptr, s);
       break;
-    case 4: st = exec_fft(c, c->d_x, CUFFT_INVERSE, s); break;
+    case 4: if (!c->fused_fft) st = exec_fft(c, c->d_x, CUFFT_INVERSE, s); break;
   }
   cudaGraph_t graph = nullptr;
   cudaError_t e = cudaStreamEndCapture(s, &graph);

@@ -1,0 +1,383 @@
+// Fused hybrid-space data consistency: forward 2-D DFT over (y, z), hard DC on the sampled
+// lines, inverse 2-D DFT, for one (x, volume) plane at a time with the plane held in shared
+// memory.  One HBM read and one write of the iterate per iteration, against two of each per
+// cuFFT pass plus the DC pass (signal_model.rs:34-79 with the x-transform cancelled, see the
+// hybrid-space identity; hard_project lib.rs:392-406 on the sampled lines).
+//
+// Each axis of length N = N1 * N2 is a four-step transform in place: N2 register DFTs of
+// length N1 (stride N2) with twiddles W_N^{n2 k1}, then N1 register DFTs of length N2; the
+// spectrum is left in the permuted order p = N2 (k mod N1) + k / N1, which the DC indexes
+// directly and the inverse (the same steps mirrored) consumes.  Register DFTs of length
+// 2, 3, 4, 6, 8, 12, 16 are nested Cooley-Tukey with FP64-computed twiddle tables.
+// Forward and inverse are unnormalised like cuFFT's; the residual sum |F x - yhat|^2 is
+// accumulated in FP64 per CTA (fixed plane order) for the deterministic finalize kernel.
+#include <cmath>
+#include <cstdio>
+#include <vector>
+#include <algorithm>
+
+#include "llr_common.cuh"
+#include "llr_internal.h"
+
+namespace llr {
+
+namespace {
+
+constexpr int kFftThreads = 512;
+
+__host__ __device__ inline size_t align16b(size_t x) { return (x + 15) & ~size_t(15); }
+
+// Twiddle-table layout in shared memory (float2 entries): W_ny^j, W_nz^j, then W_R^j for the
+// register sizes 16, 12, 8, 6 (W_4, W_3, W_2 are exact constants).
+struct FftTab {
+  int off_y, off_z, off_16, off_12, off_8, off_6, total;
+};
+
+__host__ __device__ inline FftTab fft_tab(int ny, int nz) {
+  FftTab t;
+  t.off_y = 0;
+  t.off_z = ny;
+  t.off_16 = ny + nz;
+  t.off_12 = t.off_16 + 16;
+  t.off_8 = t.off_12 + 12;
+  t.off_6 = t.off_8 + 8;
+  t.total = t.off_6 + 6;
+  return t;
+}
+
+// x * W where W = tw (forward) or conj(tw) (inverse)
+template <int DIR>
+__device__ __forceinline__ float2 twmul(float2 x, float2 tw) {
+  return DIR > 0 ? cmul(x, tw) : cmul_bc(x, tw);
+}
+
+// -i * x (forward) / +i * x (inverse)
+template <int DIR>
+__device__ __forceinline__ float2 rot(float2 x) {
+  return DIR > 0 ? make_float2(x.y, -x.x) : make_float2(-x.y, x.x);
+}
+
+template <int R, int DIR>
+struct Dft;
+
+template <int DIR>
+struct Dft<1, DIR> {
+  __device__ __forceinline__ static void run(float2* v, const float2*) {}
+};
+
+template <int DIR>
+struct Dft<2, DIR> {
+  __device__ __forceinline__ static void run(float2* v, const float2*) {
+    const float2 a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  }
+};
+
+template <int DIR>
+struct Dft<3, DIR> {
+  __device__ __forceinline__ static void run(float2* v, const float2*) {
+    const float s = 0.86602540378443864676f;   // sin(2 pi / 3)
+    const float2 a = v[0], b = v[1], c = v[2];
+    const float2 t1 = cadd(b, c);
+    const float2 t2 = make_float2(a.x - 0.5f * t1.x, a.y - 0.5f * t1.y);
+    const float2 t3 = cscale(csub(b, c), s);
+    const float2 r = rot<DIR>(t3);   // -i s (b - c) forward
+    v[0] = cadd(a, t1);
+    v[1] = cadd(t2, r);
+    v[2] = csub(t2, r);
+  }
+};
+
+template <int DIR>
+struct Dft<4, DIR> {
+  __device__ __forceinline__ static void run(float2* v, const float2*) {
+    const float2 a = v[0], b = v[1], c = v[2], d = v[3];
+    const float2 s0 = cadd(a, c), s1 = csub(a, c), s2 = cadd(b, d), s3 = rot<DIR>(csub(b, d));
+    v[0] = cadd(s0, s2);
+    v[2] = csub(s0, s2);
+    v[1] = cadd(s1, s3);
+    v[3] = csub(s1, s3);
+  }
+};
+
+// R = R1 * R2 Cooley-Tukey in registers: input natural order n = R2 n1 + n2, output natural
+// order k = k1 + R1 k2.  w: table of W_R^j, j < R.
+template <int R1, int R2, int DIR>
+__device__ __forceinline__ void dft_ct(float2* v, const float2* w, const float2* w1, const float2* w2) {
+  constexpr int R = R1 * R2;
+  float2 a[R];
+#pragma unroll
+  for (int n2 = 0; n2 < R2; ++n2) {
+    float2 t[R1];
+#pragma unroll
+    for (int n1 = 0; n1 < R1; ++n1) t[n1] = v[R2 * n1 + n2];
+    Dft<R1, DIR>::run(t, w1);
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) a[k1 * R2 + n2] = ((n2 * k1) % R == 0) ? t[k1] : twmul<DIR>(t[k1], w[(n2 * k1) % R]);
+  }
+#pragma unroll
+  for (int k1 = 0; k1 < R1; ++k1) {
+    float2 t[R2];
+#pragma unroll
+    for (int n2 = 0; n2 < R2; ++n2) t[n2] = a[k1 * R2 + n2];
+    Dft<R2, DIR>::run(t, w2);
+#pragma unroll
+    for (int k2 = 0; k2 < R2; ++k2) v[k1 + R1 * k2] = t[k2];
+  }
+}
+
+template <int DIR>
+struct Dft<6, DIR> {
+  __device__ __forceinline__ static void run(float2* v, const float2* w) { dft_ct<3, 2, DIR>(v, w, nullptr, nullptr); }
+};
+template <int DIR>
+struct Dft<8, DIR> {
+  __device__ __forceinline__ static void run(float2* v, const float2* w) { dft_ct<4, 2, DIR>(v, w, nullptr, nullptr); }
+};
+template <int DIR>
+struct Dft<12, DIR> {
+  __device__ __forceinline__ static void run(float2* v, const float2* w) { dft_ct<4, 3, DIR>(v, w, nullptr, nullptr); }
+};
+template <int DIR>
+struct Dft<16, DIR> {
+  __device__ __forceinline__ static void run(float2* v, const float2* w) { dft_ct<4, 4, DIR>(v, w, nullptr, nullptr); }
+};
+
+__device__ __forceinline__ const float2* small_tab(const float2* tw, const FftTab& T, int R) {
+  switch (R) {
+    case 16: return tw + T.off_16;
+    case 12: return tw + T.off_12;
+    case 8: return tw + T.off_8;
+    case 6: return tw + T.off_6;
+    default: return tw;
+  }
+}
+
+// One pass over every transform of an axis: B transforms (batch stride bs), each of length
+// N = N1 N2 with element stride es.  STEP 0: DFTs of length R = N1 over n1 (stride N2), then
+// twiddles; STEP 1: DFTs of length R = N2 over contiguous positions.  Forward order: 0 then 1;
+// inverse: 1 then 0 (twiddles before the DFT).
+template <int R, int DIR, int STEP>
+__device__ __forceinline__ void axis_pass(float2* s, int B, int bs, int es, int N1, int N2, const float2* wN, int N,
+                                          const float2* wR) {
+  const int J = STEP == 0 ? N2 : N1;   // transforms of length R per batch entry
+  const int tasks = B * J;
+  for (int t = threadIdx.x; t < tasks; t += blockDim.x) {
+    const int b = t % B, j = t / B;
+    float2* base = s + (long long)b * bs;
+    float2 v[R];
+    if (STEP == 0) {   // j = n2; elements at N2 n1 + n2
+#pragma unroll
+      for (int i = 0; i < R; ++i) v[i] = base[(N2 * i + j) * es];
+      // twiddle W_N^{n2 k1}, n2 k1 < N (before the inverse DFT, after the forward one)
+      if (DIR < 0) {
+#pragma unroll
+        for (int i = 1; i < R; ++i) v[i] = twmul<DIR>(v[i], wN[j * i]);
+      }
+      Dft<R, DIR>::run(v, wR);
+      if (DIR > 0) {
+#pragma unroll
+        for (int i = 1; i < R; ++i) v[i] = twmul<DIR>(v[i], wN[j * i]);
+      }
+#pragma unroll
+      for (int i = 0; i < R; ++i) base[(N2 * i + j) * es] = v[i];
+    } else {           // j = k1; elements at N2 k1 + n2
+#pragma unroll
+      for (int i = 0; i < R; ++i) v[i] = base[(N2 * j + i) * es];
+      Dft<R, DIR>::run(v, wR);
+#pragma unroll
+      for (int i = 0; i < R; ++i) base[(N2 * j + i) * es] = v[i];
+    }
+  }
+}
+
+template <int DIR, int STEP>
+__device__ void axis_dispatch(float2* s, int B, int bs, int es, int N1, int N2, const float2* wN, int N,
+                              const float2* tw, const FftTab& T) {
+  const int R = STEP == 0 ? N1 : N2;
+  const float2* wR = small_tab(tw, T, R);
+  switch (R) {
+    case 2: axis_pass<2, DIR, STEP>(s, B, bs, es, N1, N2, wN, N, wR); break;
+    case 3: axis_pass<3, DIR, STEP>(s, B, bs, es, N1, N2, wN, N, wR); break;
+    case 4: axis_pass<4, DIR, STEP>(s, B, bs, es, N1, N2, wN, N, wR); break;
+    case 6: axis_pass<6, DIR, STEP>(s, B, bs, es, N1, N2, wN, N, wR); break;
+    case 8: axis_pass<8, DIR, STEP>(s, B, bs, es, N1, N2, wN, N, wR); break;
+    case 12: axis_pass<12, DIR, STEP>(s, B, bs, es, N1, N2, wN, N, wR); break;
+    case 16: axis_pass<16, DIR, STEP>(s, B, bs, es, N1, N2, wN, N, wR); break;
+    default: break;
+  }
+}
+
+__device__ __forceinline__ int perm_pos(int k, int N1, int N2) { return N2 * (k % N1) + k / N1; }
+
+struct FftDcArgs {
+  float2* u;                 // planar iterate: plane (ix, q) at ny * nz * (ix + nx * q)
+  const float2* yhat;        // per volume q: nx x L_q, x-major (line index fastest)
+  const int* pos;            // sampled (ky + ny kz) per line
+  const long long* off;      // line offsets per volume (nq + 1)
+  const float2* twiddle;     // FftTab entries
+  double* partials;          // one FP64 residual per CTA
+  int nx, ny, nz, nq;
+  int y1, y2, z1, z2;        // ny = y1 y2, nz = z1 z2
+  int pitch;                 // odd row pitch of the shared plane
+};
+
+__global__ void __launch_bounds__(kFftThreads, 1) fft_dc_kernel(FftDcArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const FftTab T = fft_tab(a.ny, a.nz);
+  float2* tw = reinterpret_cast<float2*>(smem);
+  double* red = reinterpret_cast<double*>(smem + align16b(sizeof(float2) * T.total));
+  float2* s = reinterpret_cast<float2*>(smem + align16b(sizeof(float2) * T.total) + 32 * sizeof(double));
+  const int tid = threadIdx.x;
+  for (int i = tid; i < T.total; i += blockDim.x) tw[i] = a.twiddle[i];
+  const int ny = a.ny, nz = a.nz, P = a.pitch;
+  const long long nyz = (long long)ny * nz;
+  const long long planes = (long long)a.nx * a.nq;
+  const int dz = (int)blockDim.x / ny, dy = (int)blockDim.x - dz * ny;   // per-stride (z, y) step
+  double err = 0.0;
+  for (long long pl = blockIdx.x; pl < planes; pl += gridDim.x) {
+    const int q = (int)(pl / a.nx), ix = (int)(pl - (long long)q * a.nx);
+    float2* g = a.u + pl * nyz;
+    __syncthreads();   // previous plane stored, twiddles visible
+    {   // asynchronous 8-byte copies: every element in flight at once, no register staging
+      int z = tid / ny, y = tid - (tid / ny) * ny;
+      for (int e = tid; e < ny * nz; e += blockDim.x) {
+        const unsigned dst = (unsigned)__cvta_generic_to_shared(s + z * P + y);
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(g + e) : "memory");
+        y += dy;
+        z += dz;
+        if (y >= ny) { y -= ny; ++z; }
+      }
+      asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
+    }
+    __syncthreads();
+    // forward: y axis (rows, element stride 1, batch stride P), then z axis (columns)
+    axis_dispatch<1, 0>(s, nz, P, 1, a.y1, a.y2, tw + T.off_y, ny, tw, T);
+    __syncthreads();
+    axis_dispatch<1, 1>(s, nz, P, 1, a.y1, a.y2, tw + T.off_y, ny, tw, T);
+    __syncthreads();
+    axis_dispatch<1, 0>(s, ny, 1, P, a.z1, a.z2, tw + T.off_z, nz, tw, T);
+    __syncthreads();
+    axis_dispatch<1, 1>(s, ny, 1, P, a.z1, a.z2, tw + T.off_z, nz, tw, T);
+    __syncthreads();
+    // hard DC on the sampled lines of this plane
+    {
+      const long long o0 = a.off[q], L = a.off[q + 1] - o0;
+      const float2* yq = a.yhat + o0 * a.nx + (long long)ix * L;
+      const int* pq = a.pos + o0;
+      for (long long l = tid; l < L; l += blockDim.x) {
+        const int p = pq[l];
+        const int ky = p % ny, kz = p / ny;
+        const int at = perm_pos(kz, a.z1, a.z2) * P + perm_pos(ky, a.y1, a.y2);
+        const float2 yv = yq[l];
+        const float2 uv = s[at];
+        const double dx = (double)uv.x - (double)yv.x, dy = (double)uv.y - (double)yv.y;
+        err += dx * dx + dy * dy;
+        s[at] = yv;
+      }
+    }
+    __syncthreads();
+    // inverse: z axis then y axis, each mirrored (step 1 then step 0)
+    axis_dispatch<-1, 1>(s, ny, 1, P, a.z1, a.z2, tw + T.off_z, nz, tw, T);
+    __syncthreads();
+    axis_dispatch<-1, 0>(s, ny, 1, P, a.z1, a.z2, tw + T.off_z, nz, tw, T);
+    __syncthreads();
+    axis_dispatch<-1, 1>(s, nz, P, 1, a.y1, a.y2, tw + T.off_y, ny, tw, T);
+    __syncthreads();
+    axis_dispatch<-1, 0>(s, nz, P, 1, a.y1, a.y2, tw + T.off_y, ny, tw, T);
+    __syncthreads();
+    {
+      int z = tid / ny, y = tid - (tid / ny) * ny;
+      for (int e = tid; e < ny * nz; e += blockDim.x) {
+        g[e] = s[z * P + y];
+        y += dy;
+        z += dz;
+        if (y >= ny) { y -= ny; ++z; }
+      }
+    }
+  }
+  // deterministic CTA reduction of the residual
+  for (int o = 16; o > 0; o >>= 1) err += __shfl_xor_sync(0xffffffffu, err, o);
+  __syncthreads();
+  if ((tid & 31) == 0) red[tid >> 5] = err;
+  __syncthreads();
+  if (tid == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    a.partials[blockIdx.x] = t;
+  }
+}
+
+bool split_len(int n, int& n1, int& n2) {
+  static const int R[] = {16, 12, 8, 6, 4, 3, 2};
+  int best = -1;
+  for (int a : R)
+    for (int b : R)
+      if (a * b == n) {
+        const int bal = std::abs(a - b);
+        if (best < 0 || bal < best) { best = bal; n1 = a; n2 = b; }
+      }
+  return best >= 0;
+}
+
+size_t fft_dc_smem(int ny, int nz, int pitch) {
+  const FftTab T = fft_tab(ny, nz);
+  return align16b(sizeof(float2) * T.total) + 32 * sizeof(double) + sizeof(float2) * (size_t)pitch * nz;
+}
+
+}  // namespace
+
+bool fft_dc_supported(int ny, int nz) {
+  int a, b, c, d;
+  if (!split_len(ny, a, b) || !split_len(nz, c, d)) return false;
+  return fft_dc_smem(ny, nz, ny | 1) <= 227 * 1024;
+}
+
+// FP64 twiddle table for fft_dc_kernel (FftTab layout), uploaded once per context.
+std::vector<float2> fft_dc_twiddles(int ny, int nz) {
+  const FftTab T = fft_tab(ny, nz);
+  std::vector<float2> h((size_t)T.total);
+  auto fill = [&](int off, int N) {
+    for (int j = 0; j < N; ++j) {
+      const double ang = -2.0 * M_PI * (double)j / (double)N;
+      h[(size_t)off + j] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+    }
+  };
+  fill(T.off_y, ny);
+  fill(T.off_z, nz);
+  fill(T.off_16, 16);
+  fill(T.off_12, 12);
+  fill(T.off_8, 8);
+  fill(T.off_6, 6);
+  return h;
+}
+
+int fft_dc_grid(int ny, int nz) {
+  int dev = 0, nsm = 0, smem_sm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess) return 0;
+  const int per = std::max(1, std::min(4, smem_sm / (int)(fft_dc_smem(ny, nz, ny | 1) + 1024)));
+  return nsm * per;
+}
+
+int launch_fft_dc(float2* u, const float2* yhat, const int* pos, const long long* off, const float2* twiddle,
+                  const Geom& g, double* partials, int grid, cudaStream_t s) {
+  FftDcArgs a;
+  a.u = u; a.yhat = yhat; a.pos = pos; a.off = off; a.twiddle = twiddle; a.partials = partials;
+  a.nx = g.nx; a.ny = g.ny; a.nz = g.nz; a.nq = g.nq;
+  if (!split_len(g.ny, a.y1, a.y2) || !split_len(g.nz, a.z1, a.z2))
+    return set_error(LLR_ERR_UNSUPPORTED, "fused FFT: %d x %d does not factor into register DFTs", g.ny, g.nz);
+  a.pitch = g.ny | 1;
+  const size_t smem = fft_dc_smem(g.ny, g.nz, a.pitch);
+  LLR_CUDA_TRY(cudaFuncSetAttribute(fft_dc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  LLR_CUDA_TRY(cudaFuncSetAttribute(fft_dc_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  if (grid < 1) return set_error(LLR_ERR_INVALID, "fused FFT: empty grid");
+  note_launch();
+  fft_dc_kernel<<<grid, kFftThreads, smem, s>>>(a);
+  LLR_CUDA_TRY(cudaGetLastError());
+  return LLR_OK;
+}
+
+}  // namespace llr

@@ -59,6 +59,11 @@ inline long long prox_gram_stride(int n) {
   return p > f ? p : f;
 }
 
+bool fft_dc_supported(int ny, int nz);
+std::vector<float2> fft_dc_twiddles(int ny, int nz);
+int fft_dc_grid(int ny, int nz);
+int launch_fft_dc(float2* u, const float2* yhat, const int* pos, const long long* off, const float2* twiddle,
+                  const Geom& g, double* partials, int grid, cudaStream_t s);
 int launch_llr_eig_warp(const ProxOp& op, long long nblocks, cudaStream_t stream);
 
 int launch_llr_prox(const BlockSource& src, const ProxOp& op, cudaStream_t stream);
@@ -119,6 +124,9 @@ struct llr_ctx {
   bool have_kspace;
   bool have_image;
   bool hybrid;              // line-structured measurements: x-transform eliminated
+  bool fused_fft;           // hybrid and the (y, z) plane fits fft_dc_kernel
+  int fft_grid;             // fft_dc_kernel CTAs (= residual partials)
+  float2* d_fft_tw;         // fft_dc_kernel twiddle table
   float load_scale;         // 1 / N_t
   // device buffers
   float2* d_x;              // iterate (planar, raw convention)

@@ -55,7 +55,8 @@ class llr_config(C.Structure):
         ("device", C.c_int32),
         ("eig_solver", C.c_int32),
         ("gram_mode", C.c_int32),
-        ("reserved", C.c_int32 * 5),
+        ("fft_mode", C.c_int32),
+        ("reserved", C.c_int32 * 4),
     ]
 
 

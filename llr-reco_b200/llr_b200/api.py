@@ -116,6 +116,7 @@ class ReconParams:
     device: int = 0
     eig_solver: int = 0
     gram_mode: int = 0
+    fft_mode: int = 0
 
     def to_c(self) -> L.llr_config:
         c = L.llr_config()
@@ -136,6 +137,7 @@ class ReconParams:
         c.device = int(self.device)
         c.eig_solver = int(self.eig_solver)
         c.gram_mode = int(self.gram_mode)
+        c.fft_mode = int(self.fft_mode)
         return c
 
 

@@ -30,7 +30,7 @@ def oracle_cfg(bs, mode, rank=0, lam=0.0, seed=0, **kw):
 
 
 def run_both(y, bs, mode, n_iter, rank=2, lam_rel=0.02, seed=5, lin=None, wavelet=None, subspace=None,
-             max_shift=None, eig_solver=0, gram_mode=0):
+             max_shift=None, eig_solver=0, gram_mode=0, fft_mode=0):
     nx, ny, nz, nq = y.shape
     ocfg = oracle_cfg(bs, "hard" if mode == L.LLR_PROX_HARD_RANK else "soft", rank=rank, seed=seed,
                       max_rand_shift=max_shift)
@@ -46,7 +46,7 @@ def run_both(y, bs, mode, n_iter, rank=2, lam_rel=0.02, seed=5, lin=None, wavele
     if wavelet is not None:
         ocfg.wavelet_alpha, ocfg.wavelet_moments, ocfg.wavelet_levels = wavelet
     p = ReconParams(vol_size=(nx, ny, nz), nq=nq, block_size=bs, prox_mode=mode, rank=rank, lam=lam, seed=seed,
-                    max_rand_shift=max_shift, eig_solver=eig_solver, gram_mode=gram_mode,
+                    max_rand_shift=max_shift, eig_solver=eig_solver, gram_mode=gram_mode, fft_mode=fft_mode,
                     subspace_rank=0 if subspace is None else subspace.shape[1])
     if wavelet is not None:
         p.wavelet_alpha, p.wavelet_moments, p.wavelet_levels = wavelet
@@ -97,6 +97,32 @@ def test_soft_c2_like(gpu, eig_solver, gram_mode):
     gx, ox, gh, oh, _ = run_both(d.y, (6, 6, 6), L.LLR_PROX_SOFT_THRESH, 4, eig_solver=eig_solver,
                                  gram_mode=gram_mode)
     check(gx, ox, gh, oh)
+
+
+@pytest.mark.parametrize("vol,fft_mode", [((16, 24, 12), 0), ((16, 24, 12), 1), ((6, 48, 32), 0)])
+def test_fused_fft_dc(gpu, vol, fft_mode):
+    """Hybrid path with the fused per-plane FFT + DC + inverse FFT kernel (fft_mode 0; plane
+    sizes 24 = 6 x 4, 12 = 4 x 3, 48 = 8 x 6, 32 = 8 x 4) and with cuFFT passes (fft_mode 1)."""
+    d = dataset(vol, 7, accel=4.0, centre=4)
+    gx, ox, gh, oh, _ = run_both(d.y, (4, 4, 4), L.LLR_PROX_SOFT_THRESH, 4, fft_mode=fft_mode)
+    check(gx, ox, gh, oh)
+
+
+def test_fused_fft_dc_c2_plane(gpu):
+    """The 192 x 96 (y, z) plane of the production configuration (16 x 12 and 12 x 8 register
+    DFTs), fused against cuFFT on the same data."""
+    d = dataset((6, 192, 96), 5, accel=8.0, centre=8)
+    out = {}
+    for mode in (0, 1):
+        p = ReconParams(vol_size=(6, 192, 96), nq=5, block_size=(6, 6, 6), prox_mode=L.LLR_PROX_SOFT_THRESH,
+                        lam=0.5, seed=3, fft_mode=mode)
+        with ReconContext(p) as ctx:
+            ctx.upload_kspace(d.y)
+            ctx.init_zero_filled()
+            h = ctx.iterate(3)
+            out[mode] = (ctx.download_image(), np.asarray(h))
+    assert rel_err(out[0][0], out[1][0]) < 2e-6
+    np.testing.assert_allclose(out[0][1], out[1][1], rtol=2e-6)
 
 
 def test_element_wise_sampling_path(gpu):
