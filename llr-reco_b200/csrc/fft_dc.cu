@@ -101,10 +101,36 @@ struct Dft<4, DIR> {
   }
 };
 
+// W_R^m = e^{-2 pi i m / R} for the register DFTs, evaluated at compile time from the Taylor
+// series of cos and sin in double precision (|x| <= 2 pi, 30 terms).
+constexpr double kTwoPi = 6.283185307179586476925286766559;
+constexpr double taylor_cos(double x) {
+  double t = 1.0, s = 1.0;
+  for (int k = 1; k < 30; ++k) { t *= -x * x / ((2.0 * k - 1.0) * (2.0 * k)); s += t; }
+  return s;
+}
+constexpr double taylor_sin(double x) {
+  double t = x, s = x;
+  for (int k = 1; k < 30; ++k) { t *= -x * x / ((2.0 * k) * (2.0 * k + 1.0)); s += t; }
+  return s;
+}
+template <int R>
+struct TwTab {
+  float re[R], im[R];
+  constexpr TwTab() : re(), im() {
+    for (int m = 0; m < R; ++m) {
+      re[m] = (float)taylor_cos(kTwoPi * m / R);
+      im[m] = (float)-taylor_sin(kTwoPi * m / R);
+    }
+  }
+};
+template <int R>
+__device__ constexpr TwTab<R> kTw = TwTab<R>();
+
 // R = R1 * R2 Cooley-Tukey in registers: input natural order n = R2 n1 + n2, output natural
-// order k = k1 + R1 k2.  w: table of W_R^j, j < R.
+// order k = k1 + R1 k2; twiddles W_R^{n2 k1} are compile-time constants.
 template <int R1, int R2, int DIR>
-__device__ __forceinline__ void dft_ct(float2* v, const float2* w, const float2* w1, const float2* w2) {
+__device__ __forceinline__ void dft_ct(float2* v, const float2*, const float2* w1, const float2* w2) {
   constexpr int R = R1 * R2;
   float2 a[R];
 #pragma unroll
@@ -114,7 +140,10 @@ __device__ __forceinline__ void dft_ct(float2* v, const float2* w, const float2*
     for (int n1 = 0; n1 < R1; ++n1) t[n1] = v[R2 * n1 + n2];
     Dft<R1, DIR>::run(t, w1);
 #pragma unroll
-    for (int k1 = 0; k1 < R1; ++k1) a[k1 * R2 + n2] = ((n2 * k1) % R == 0) ? t[k1] : twmul<DIR>(t[k1], w[(n2 * k1) % R]);
+    for (int k1 = 0; k1 < R1; ++k1) {
+      const int m = (n2 * k1) % R;
+      a[k1 * R2 + n2] = m == 0 ? t[k1] : twmul<DIR>(t[k1], make_float2(kTw<R>.re[m], kTw<R>.im[m]));
+    }
   }
 #pragma unroll
   for (int k1 = 0; k1 < R1; ++k1) {
@@ -223,15 +252,91 @@ struct FftDcArgs {
   int pitch;                 // odd row pitch of the shared plane
 };
 
-__global__ void __launch_bounds__(kFftThreads, 1) fft_dc_kernel(FftDcArgs a) {
+// Passes of one axis with every size a compile-time constant (hot plane shapes).
+template <int DIR, int STEP, int B, int BS, int ES, int N1, int N2, int NT>
+__device__ __forceinline__ void axis_pass_fixed(float2* s, const float2* wN) {
+  constexpr int R = STEP == 0 ? N1 : N2;
+  constexpr int J = STEP == 0 ? N2 : N1;
+  constexpr int TASKS = B * J;
+#pragma unroll 1
+  for (int t = threadIdx.x; t < TASKS; t += NT) {
+    const int b = t % B, j = t / B;
+    float2* base = s + b * BS + (STEP == 0 ? j : N2 * j) * ES;
+    float2 v[R];
+#pragma unroll
+    for (int i = 0; i < R; ++i) v[i] = base[(STEP == 0 ? N2 * i : i) * ES];
+    if (STEP == 0 && DIR < 0) {
+#pragma unroll
+      for (int i = 1; i < R; ++i) v[i] = twmul<DIR>(v[i], wN[j * i]);
+    }
+    Dft<R, DIR>::run(v, nullptr);
+    if (STEP == 0 && DIR > 0) {
+#pragma unroll
+      for (int i = 1; i < R; ++i) v[i] = twmul<DIR>(v[i], wN[j * i]);
+    }
+#pragma unroll
+    for (int i = 0; i < R; ++i) base[(STEP == 0 ? N2 * i : i) * ES] = v[i];
+  }
+}
+
+// Plane geometry with run-time sizes (any shape split_len accepts).
+struct GeoRt {
+  int ny, nz, y1, y2, z1, z2, P;
+  __device__ void forward(float2* s, const float2* tw, const FftTab& T) const {
+    axis_dispatch<1, 0>(s, nz, P, 1, y1, y2, tw + T.off_y, ny, tw, T);
+    __syncthreads();
+    axis_dispatch<1, 1>(s, nz, P, 1, y1, y2, tw + T.off_y, ny, tw, T);
+    __syncthreads();
+    axis_dispatch<1, 0>(s, ny, 1, P, z1, z2, tw + T.off_z, nz, tw, T);
+    __syncthreads();
+    axis_dispatch<1, 1>(s, ny, 1, P, z1, z2, tw + T.off_z, nz, tw, T);
+  }
+  __device__ void inverse(float2* s, const float2* tw, const FftTab& T) const {
+    axis_dispatch<-1, 1>(s, ny, 1, P, z1, z2, tw + T.off_z, nz, tw, T);
+    __syncthreads();
+    axis_dispatch<-1, 0>(s, ny, 1, P, z1, z2, tw + T.off_z, nz, tw, T);
+    __syncthreads();
+    axis_dispatch<-1, 1>(s, nz, P, 1, y1, y2, tw + T.off_y, ny, tw, T);
+    __syncthreads();
+    axis_dispatch<-1, 0>(s, nz, P, 1, y1, y2, tw + T.off_y, ny, tw, T);
+  }
+};
+
+// Plane geometry with compile-time sizes: ny = Y1 Y2, nz = Z1 Z2, NT threads.
+template <int Y1, int Y2, int Z1, int Z2, int NT>
+struct GeoFixed {
+  static constexpr int NY = Y1 * Y2, NZ = Z1 * Z2, PP = NY | 1;
+  int ny = NY, nz = NZ, y1 = Y1, y2 = Y2, z1 = Z1, z2 = Z2, P = PP;
+  __device__ void forward(float2* s, const float2* tw, const FftTab& T) const {
+    axis_pass_fixed<1, 0, NZ, PP, 1, Y1, Y2, NT>(s, tw + T.off_y);
+    __syncthreads();
+    axis_pass_fixed<1, 1, NZ, PP, 1, Y1, Y2, NT>(s, tw + T.off_y);
+    __syncthreads();
+    axis_pass_fixed<1, 0, NY, 1, PP, Z1, Z2, NT>(s, tw + T.off_z);
+    __syncthreads();
+    axis_pass_fixed<1, 1, NY, 1, PP, Z1, Z2, NT>(s, tw + T.off_z);
+  }
+  __device__ void inverse(float2* s, const float2* tw, const FftTab& T) const {
+    axis_pass_fixed<-1, 1, NY, 1, PP, Z1, Z2, NT>(s, tw + T.off_z);
+    __syncthreads();
+    axis_pass_fixed<-1, 0, NY, 1, PP, Z1, Z2, NT>(s, tw + T.off_z);
+    __syncthreads();
+    axis_pass_fixed<-1, 1, NZ, PP, 1, Y1, Y2, NT>(s, tw + T.off_y);
+    __syncthreads();
+    axis_pass_fixed<-1, 0, NZ, PP, 1, Y1, Y2, NT>(s, tw + T.off_y);
+  }
+};
+
+template <class Geo>
+__device__ __forceinline__ void fft_dc_body(const FftDcArgs& a, const Geo& geo) {
   extern __shared__ __align__(16) unsigned char smem[];
-  const FftTab T = fft_tab(a.ny, a.nz);
+  const int ny = geo.ny, nz = geo.nz, P = geo.P;
+  const FftTab T = fft_tab(ny, nz);
   float2* tw = reinterpret_cast<float2*>(smem);
   double* red = reinterpret_cast<double*>(smem + align16b(sizeof(float2) * T.total));
   float2* s = reinterpret_cast<float2*>(smem + align16b(sizeof(float2) * T.total) + 32 * sizeof(double));
   const int tid = threadIdx.x;
   for (int i = tid; i < T.total; i += blockDim.x) tw[i] = a.twiddle[i];
-  const int ny = a.ny, nz = a.nz, P = a.pitch;
   const long long nyz = (long long)ny * nz;
   const long long planes = (long long)a.nx * a.nq;
   const int dz = (int)blockDim.x / ny, dy = (int)blockDim.x - dz * ny;   // per-stride (z, y) step
@@ -253,13 +358,7 @@ __global__ void __launch_bounds__(kFftThreads, 1) fft_dc_kernel(FftDcArgs a) {
     }
     __syncthreads();
     // forward: y axis (rows, element stride 1, batch stride P), then z axis (columns)
-    axis_dispatch<1, 0>(s, nz, P, 1, a.y1, a.y2, tw + T.off_y, ny, tw, T);
-    __syncthreads();
-    axis_dispatch<1, 1>(s, nz, P, 1, a.y1, a.y2, tw + T.off_y, ny, tw, T);
-    __syncthreads();
-    axis_dispatch<1, 0>(s, ny, 1, P, a.z1, a.z2, tw + T.off_z, nz, tw, T);
-    __syncthreads();
-    axis_dispatch<1, 1>(s, ny, 1, P, a.z1, a.z2, tw + T.off_z, nz, tw, T);
+    geo.forward(s, tw, T);
     __syncthreads();
     // hard DC on the sampled lines of this plane
     {
@@ -269,23 +368,17 @@ __global__ void __launch_bounds__(kFftThreads, 1) fft_dc_kernel(FftDcArgs a) {
       for (long long l = tid; l < L; l += blockDim.x) {
         const int p = pq[l];
         const int ky = p % ny, kz = p / ny;
-        const int at = perm_pos(kz, a.z1, a.z2) * P + perm_pos(ky, a.y1, a.y2);
+        const int at = perm_pos(kz, geo.z1, geo.z2) * P + perm_pos(ky, geo.y1, geo.y2);
         const float2 yv = yq[l];
         const float2 uv = s[at];
-        const double dx = (double)uv.x - (double)yv.x, dy = (double)uv.y - (double)yv.y;
-        err += dx * dx + dy * dy;
+        const double dx = (double)uv.x - (double)yv.x, dy2 = (double)uv.y - (double)yv.y;
+        err += dx * dx + dy2 * dy2;
         s[at] = yv;
       }
     }
     __syncthreads();
     // inverse: z axis then y axis, each mirrored (step 1 then step 0)
-    axis_dispatch<-1, 1>(s, ny, 1, P, a.z1, a.z2, tw + T.off_z, nz, tw, T);
-    __syncthreads();
-    axis_dispatch<-1, 0>(s, ny, 1, P, a.z1, a.z2, tw + T.off_z, nz, tw, T);
-    __syncthreads();
-    axis_dispatch<-1, 1>(s, nz, P, 1, a.y1, a.y2, tw + T.off_y, ny, tw, T);
-    __syncthreads();
-    axis_dispatch<-1, 0>(s, nz, P, 1, a.y1, a.y2, tw + T.off_y, ny, tw, T);
+    geo.inverse(s, tw, T);
     __syncthreads();
     {
       int z = tid / ny, y = tid - (tid / ny) * ny;
@@ -307,6 +400,17 @@ __global__ void __launch_bounds__(kFftThreads, 1) fft_dc_kernel(FftDcArgs a) {
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
     a.partials[blockIdx.x] = t;
   }
+}
+
+__global__ void __launch_bounds__(kFftThreads, 1) fft_dc_kernel(FftDcArgs a) {
+  GeoRt geo;
+  geo.ny = a.ny; geo.nz = a.nz; geo.y1 = a.y1; geo.y2 = a.y2; geo.z1 = a.z1; geo.z2 = a.z2; geo.P = a.pitch;
+  fft_dc_body(a, geo);
+}
+
+template <int Y1, int Y2, int Z1, int Z2, int NT>
+__global__ void __launch_bounds__(NT, 1) fft_dc_fixed_kernel(FftDcArgs a) {
+  fft_dc_body(a, GeoFixed<Y1, Y2, Z1, Z2, NT>());
 }
 
 bool split_len(int n, int& n1, int& n2) {
@@ -353,12 +457,44 @@ std::vector<float2> fft_dc_twiddles(int ny, int nz) {
   return h;
 }
 
+namespace {
+
+// Compile-time instances for the hot plane shapes; every other factorable shape uses the
+// run-time kernel.  Thread counts divide every pass's task count.
+struct FftKernelChoice {
+  void (*kern)(FftDcArgs);
+  int nt, y1, y2, z1, z2;
+};
+
+FftKernelChoice choose_fft(int ny, int nz) {
+  FftKernelChoice c;
+  if (ny == 192 && nz == 96) c = {fft_dc_fixed_kernel<16, 12, 12, 8, 384>, 384, 16, 12, 12, 8};
+  else if (ny == 96 && nz == 48) c = {fft_dc_fixed_kernel<12, 8, 8, 6, 192>, 192, 12, 8, 8, 6};
+  else if (ny == 64 && nz == 64) c = {fft_dc_fixed_kernel<8, 8, 8, 8, 256>, 256, 8, 8, 8, 8};
+  else {
+    c.kern = fft_dc_kernel;
+    c.nt = kFftThreads;
+    split_len(ny, c.y1, c.y2);
+    split_len(nz, c.z1, c.z2);
+  }
+  return c;
+}
+
+}  // namespace
+
 int fft_dc_grid(int ny, int nz) {
-  int dev = 0, nsm = 0, smem_sm = 0;
+  int dev = 0, nsm = 0, smem_sm = 0, regs_sm = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return 0;
   if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
   if (cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess) return 0;
-  const int per = std::max(1, std::min(4, smem_sm / (int)(fft_dc_smem(ny, nz, ny | 1) + 1024)));
+  if (cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev) != cudaSuccess) return 0;
+  const FftKernelChoice c = choose_fft(ny, nz);
+  cudaFuncAttributes fa{};
+  if (cudaFuncGetAttributes(&fa, c.kern) != cudaSuccess) return 0;
+  const int by_smem = smem_sm / (int)(fft_dc_smem(ny, nz, ny | 1) + 1024);
+  const int regs_warp = ((fa.numRegs * 32 + 255) / 256) * 256;
+  const int by_regs = regs_sm / std::max(1, regs_warp * (c.nt / 32));
+  const int per = std::max(1, std::min(4, std::min(by_smem, by_regs)));
   return nsm * per;
 }
 
@@ -367,15 +503,17 @@ int launch_fft_dc(float2* u, const float2* yhat, const int* pos, const long long
   FftDcArgs a;
   a.u = u; a.yhat = yhat; a.pos = pos; a.off = off; a.twiddle = twiddle; a.partials = partials;
   a.nx = g.nx; a.ny = g.ny; a.nz = g.nz; a.nq = g.nq;
-  if (!split_len(g.ny, a.y1, a.y2) || !split_len(g.nz, a.z1, a.z2))
-    return set_error(LLR_ERR_UNSUPPORTED, "fused FFT: %d x %d does not factor into register DFTs", g.ny, g.nz);
+  if (!fft_dc_supported(g.ny, g.nz))
+    return set_error(LLR_ERR_UNSUPPORTED, "fused FFT: %d x %d plane is not supported", g.ny, g.nz);
+  const FftKernelChoice c = choose_fft(g.ny, g.nz);
+  a.y1 = c.y1; a.y2 = c.y2; a.z1 = c.z1; a.z2 = c.z2;
   a.pitch = g.ny | 1;
   const size_t smem = fft_dc_smem(g.ny, g.nz, a.pitch);
-  LLR_CUDA_TRY(cudaFuncSetAttribute(fft_dc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  LLR_CUDA_TRY(cudaFuncSetAttribute(fft_dc_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  LLR_CUDA_TRY(cudaFuncSetAttribute(c.kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  LLR_CUDA_TRY(cudaFuncSetAttribute(c.kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   if (grid < 1) return set_error(LLR_ERR_INVALID, "fused FFT: empty grid");
   note_launch();
-  fft_dc_kernel<<<grid, kFftThreads, smem, s>>>(a);
+  c.kern<<<grid, c.nt, smem, s>>>(a);
   LLR_CUDA_TRY(cudaGetLastError());
   return LLR_OK;
 }
