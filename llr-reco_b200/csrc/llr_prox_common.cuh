@@ -39,15 +39,16 @@ __device__ __forceinline__ void block_shift(const BlockSource& s, int* sh) {
   }
 }
 
-// Voxel coordinates of row r of block `blk` (rows ordered y fastest, then z, then x:
-// the contiguous axis of the planar layout).  Corner = grid index * block + shift
-// (block.rs:122-133); every coordinate wraps modulo the volume (block.rs:20-22).
+// Voxel coordinates of row r of block `blk`.  Rows are ordered y fastest, then z, then x, and
+// so are the blocks (the planar layout's order: blocks that run at the same time share DRAM
+// pages; the order of independent blocks does not change any result).  Corner = grid index *
+// block + shift (block.rs:122-133); every coordinate wraps modulo the volume (block.rs:20-22).
 __device__ __forceinline__ void block_row_coord(const BlockSource& s, long long blk, const int* sh, int r,
                                                 int& ix, int& iy, int& iz) {
-  int gxi = (int)(blk % s.gx);
-  long long t = blk / s.gx;
-  int gyi = (int)(t % s.gy);
-  int gzi = (int)(t / s.gy);
+  int gyi = (int)(blk % s.gy);
+  long long t = blk / s.gy;
+  int gzi = (int)(t % s.gz);
+  int gxi = (int)(t / s.gz);
   int ry = r % s.by;
   int t2 = r / s.by;
   int rz = t2 % s.bz;
