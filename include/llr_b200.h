@@ -252,6 +252,37 @@ int llr_memcpy_d2h(void* dst, const void* src, size_t bytes, void* stream);
 int llr_stream_sync(void* stream);
 int llr_device_count(int32_t* n);
 
+/* ---- learned warm start: 3-D residual CNN ----------------------------------------
+ * No reference counterpart: the reference has no learned component.  A network of
+ * n_layers conv3d 3x3x3 layers (zero padding, ReLU between layers, out = in + net(in));
+ * channels[0..n_layers], channels[0] == channels[n_layers]; built layer shapes are
+ * 14->32, 32->32 and 32->14.  Activations are channels-last FP32 over a volume
+ * dims[3] (x fastest); weights are used in BF16 with FP32 accumulation, the optimizer
+ * (Adam) keeps FP32 master parameters.  Parameter order per layer: W[27][cin][cout]
+ * (tap = dx + 3 (dy + 3 dz)), then b[cout]. */
+typedef struct llr_cnn llr_cnn;
+int llr_cnn_create(int32_t n_layers, const int32_t* channels, int32_t device, uint64_t seed, llr_cnn** out);
+int llr_cnn_destroy(llr_cnn* net);
+int llr_cnn_param_count(const llr_cnn* net, int64_t* count);
+int llr_cnn_get_params(llr_cnn* net, float* host);
+int llr_cnn_set_params(llr_cnn* net, const float* host);
+int llr_cnn_get_grads(llr_cnn* net, float* host);
+int llr_cnn_forward_dev(llr_cnn* net, const float* d_in, float* d_out, const int32_t* dims, void* stream);
+/* forward, mean-squared-error loss against d_target, backward: gradients kept in the net */
+int llr_cnn_loss_grad_dev(llr_cnn* net, const float* d_in, const float* d_target, const int32_t* dims,
+                          double* loss, void* stream);
+int llr_cnn_adam_step(llr_cnn* net, float lr, float beta1, float beta2, float eps, void* stream);
+int llr_cnn_train_step_dev(llr_cnn* net, const float* d_in, const float* d_target, const int32_t* dims,
+                           float lr, double* loss, void* stream);
+/* CNN channels of subspace coefficients: chan[v][2k + {0,1}] = scale (re, im)(sum_q x[v + V q]
+ * S[q + nq k]) (dti_subspace.rs:141-166), and the image back: x = (1/scale) c S^H, or
+ * x += (1/scale) c S^H with accumulate != 0 (dti_subspace.rs:172-207).  Images in the
+ * reference layout; 1 <= srank <= 16. */
+int llr_subspace_channels_dev(const llr_cf32* d_x, const int32_t* vol, int32_t nq, const llr_cf32* d_S,
+                              int32_t srank, float scale, float* d_chan, void* stream);
+int llr_subspace_image_dev(const float* d_chan, const int32_t* vol, int32_t nq, const llr_cf32* d_S,
+                           int32_t srank, float scale, int32_t accumulate, llr_cf32* d_x, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -144,6 +144,18 @@ SIGNATURES = {
     "llr_memcpy_d2h": (C.c_int, [P, P, SZ, P]),
     "llr_stream_sync": (C.c_int, [P]),
     "llr_device_count": (C.c_int, [PI32]),
+    "llr_cnn_create": (C.c_int, [I32, PI32, I32, U64, C.POINTER(P)]),
+    "llr_cnn_destroy": (C.c_int, [P]),
+    "llr_cnn_param_count": (C.c_int, [P, C.POINTER(I64)]),
+    "llr_cnn_get_params": (C.c_int, [P, P]),
+    "llr_cnn_set_params": (C.c_int, [P, P]),
+    "llr_cnn_get_grads": (C.c_int, [P, P]),
+    "llr_cnn_forward_dev": (C.c_int, [P, P, P, PI32, P]),
+    "llr_cnn_loss_grad_dev": (C.c_int, [P, P, P, PI32, PF64, P]),
+    "llr_cnn_adam_step": (C.c_int, [P, C.c_float, C.c_float, C.c_float, C.c_float, P]),
+    "llr_cnn_train_step_dev": (C.c_int, [P, P, P, PI32, C.c_float, PF64, P]),
+    "llr_subspace_channels_dev": (C.c_int, [P, PI32, I32, P, I32, C.c_float, P, P]),
+    "llr_subspace_image_dev": (C.c_int, [P, PI32, I32, P, I32, C.c_float, I32, P, P]),
 }
 
 

@@ -125,14 +125,17 @@ def centred_fft_unitary(x: np.ndarray) -> np.ndarray:
 
 
 def make_dataset(vol, shells, accel, seed, centre=16, snr=30.0, n_ellipsoids=6,
-                 mask_fn: Optional[Callable] = None, forward: Optional[Callable] = None) -> Dataset:
+                 mask_fn: Optional[Callable] = None, forward: Optional[Callable] = None,
+                 protocol_seed: Optional[int] = None) -> Dataset:
     """Phantom, per-volume VD ky-kz mask, complex Gaussian noise at ``snr``.
 
     Noise: sigma = mean |x_true| over the object / snr, added with standard deviation sigma
-    to the real and to the imaginary part of every sampled k-space sample.
+    to the real and to the imaginary part of every sampled k-space sample.  With
+    ``protocol_seed`` the b-table (the acquisition protocol) comes from that seed and only the
+    phantom, mask and noise from ``seed``, so that many subjects share one protocol.
     """
     rng = np.random.default_rng(seed)
-    b, g = b_table(shells, rng)
+    b, g = b_table(shells, np.random.default_rng(protocol_seed) if protocol_seed is not None else rng)
     x = phantom_image(vol, b, g, rng, n_ellipsoids=n_ellipsoids)
     nx, ny, nz = vol
     nq = len(b)
