@@ -133,6 +133,13 @@ int llr_iterate_async(llr_ctx* ctx, int32_t n_iter);
 int llr_iterate_profiled(llr_ctx* ctx, int32_t n_iter, double* stage_ms, double* total_ms);
 /* Device time of n single-graph iterations (events on the context stream). */
 int llr_iterate_timed(llr_ctx* ctx, int32_t n_iter, double* total_ms);
+/* Copy of the iterate in the context's internal layout (V * nq complex), and the relative
+ * RMS distance ||x - ref|| / ||ref|| of the current iterate to such a copy taken from a
+ * context with the same configuration and k-space (the internal layout differs from the
+ * image by a per-element phase and one scale, so the ratio is that of the images).
+ * No reference counterpart: convergence measurement without host copies. */
+int llr_ctx_snapshot(llr_ctx* ctx, llr_cf32* d_dst);
+int llr_ctx_nrmse(llr_ctx* ctx, const llr_cf32* d_ref, double* nrmse);
 /* Number of this library's kernels that one captured iteration launches (cuFFT's kernels
  * are not counted).  Valid after the first llr_iterate* call; no reference counterpart. */
 int llr_ctx_kernel_launches(const llr_ctx* ctx, int32_t* per_iteration);

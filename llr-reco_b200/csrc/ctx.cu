@@ -741,6 +741,32 @@ int llr_iterate(llr_ctx* c, int32_t n, double* hist) {
   return LLR_OK;
 }
 
+int llr_ctx_snapshot(llr_ctx* c, llr_cf32* d_dst) {
+  if (!c || !d_dst) return set_error(LLR_ERR_INVALID, "null pointer");
+  if (!c->have_image) return set_error(LLR_ERR_STATE, "no image");
+  LLR_CUDA_TRY(cudaSetDevice(c->device));
+  LLR_CUDA_TRY(cudaMemcpyAsync(d_dst, c->d_x, sizeof(float2) * (size_t)c->g.V * c->g.nq, cudaMemcpyDeviceToDevice,
+                               c->stream));
+  LLR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return LLR_OK;
+}
+
+int llr_ctx_nrmse(llr_ctx* c, const llr_cf32* d_ref, double* out) {
+  if (!c || !d_ref || !out) return set_error(LLR_ERR_INVALID, "null pointer");
+  if (!c->have_image) return set_error(LLR_ERR_STATE, "no image");
+  LLR_CUDA_TRY(cudaSetDevice(c->device));
+  constexpr int nb = 512;
+  LLR_TRY(launch_diff_norm(c->d_x, (const float2*)d_ref, c->g.V * c->g.nq, c->d_partials, c->d_partials + nb, nb,
+                           c->stream));
+  std::vector<double> h(2 * nb);
+  LLR_CUDA_TRY(cudaMemcpyAsync(h.data(), c->d_partials, sizeof(double) * 2 * nb, cudaMemcpyDeviceToHost, c->stream));
+  LLR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  double d = 0.0, r = 0.0;
+  for (int i = 0; i < nb; ++i) { d += h[i]; r += h[nb + i]; }
+  *out = r > 0.0 ? std::sqrt(d / r) : INFINITY;
+  return LLR_OK;
+}
+
 int llr_ctx_kernel_launches(const llr_ctx* c, int32_t* per_iteration) {
   if (!c || !per_iteration) return set_error(LLR_ERR_INVALID, "null pointer");
   if (!c->have_graph && !c->have_stages) return set_error(LLR_ERR_STATE, "no iteration has been captured yet");

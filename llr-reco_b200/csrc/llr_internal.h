@@ -64,6 +64,8 @@ std::vector<float2> fft_dc_twiddles(int ny, int nz);
 int fft_dc_grid(int ny, int nz);
 int launch_fft_dc(float2* u, const float2* yhat, const int* pos, const long long* off, const float2* twiddle,
                   const Geom& g, double* partials, int grid, cudaStream_t s);
+int launch_diff_norm(const float2* a, const float2* b, long long n, double* part_d, double* part_b, int nblocks,
+                     cudaStream_t s);
 int launch_llr_eig_warp(const ProxOp& op, long long nblocks, cudaStream_t stream);
 
 int launch_llr_prox(const BlockSource& src, const ProxOp& op, cudaStream_t stream);

@@ -219,6 +219,23 @@ __global__ void __launch_bounds__(256) finalize_kernel(const double* partials, i
   }
 }
 
+// sum |a - b|^2 and sum |b|^2 in FP64, one pair of partials per block
+__global__ void __launch_bounds__(256) diff_norm_kernel(const float2* __restrict__ a, const float2* __restrict__ b,
+                                                        long long n, double* part_d, double* part_b) {
+  __shared__ double sh[8];
+  double d = 0.0, r = 0.0;
+  for (long long i = blockIdx.x * 256LL + threadIdx.x; i < n; i += (long long)gridDim.x * 256) {
+    const float2 u = a[i], v = b[i];
+    const double dx = (double)u.x - v.x, dy = (double)u.y - v.y;
+    d += dx * dx + dy * dy;
+    r += (double)v.x * v.x + (double)v.y * v.y;
+  }
+  double s = block_reduce_d<256>(d, sh);
+  __syncthreads();
+  double t = block_reduce_d<256>(r, sh);
+  if (threadIdx.x == 0) { part_d[blockIdx.x] = s; part_b[blockIdx.x] = t; }
+}
+
 // Per-line non-zero count along x (reference layout): one warp per (ky, kz, q) line.
 __global__ void line_nnz_kernel(const float2* __restrict__ y, long long nlines, int nx, int* cnt) {
   const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
@@ -387,6 +404,14 @@ int launch_line_nnz(const float2* y, long long nlines, int nx, int* cnt, cudaStr
   long long threads = nlines * 32;
   note_launch();
   line_nnz_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(y, nlines, nx, cnt);
+  LLR_CUDA_TRY(cudaGetLastError());
+  return LLR_OK;
+}
+
+int launch_diff_norm(const float2* a, const float2* b, long long n, double* part_d, double* part_b, int nblocks,
+                     cudaStream_t s) {
+  note_launch();
+  diff_norm_kernel<<<nblocks, 256, 0, s>>>(a, b, n, part_d, part_b);
   LLR_CUDA_TRY(cudaGetLastError());
   return LLR_OK;
 }

@@ -207,6 +207,18 @@ class ReconContext:
         check(lib.llr_iterate_profiled(self.h, int(n), st.ctypes.data_as(L.PF64), C.byref(tot)))
         return st, tot.value
 
+    def snapshot(self) -> DeviceBuffer:
+        """Device copy of the iterate in the internal layout (for nrmse())."""
+        b = DeviceBuffer(8 * int(np.prod(self.shape)))
+        check(lib.llr_ctx_snapshot(self.h, b.ptr))
+        return b
+
+    def nrmse(self, snap: DeviceBuffer) -> float:
+        """||x - ref|| / ||ref|| against a snapshot of a context with the same configuration."""
+        v = C.c_double()
+        check(lib.llr_ctx_nrmse(self.h, snap.ptr, C.byref(v)))
+        return float(v.value)
+
     @property
     def kernel_launches_per_iteration(self) -> int:
         """Library kernels (not cuFFT's) one captured iteration launches."""

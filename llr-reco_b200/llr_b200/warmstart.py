@@ -41,6 +41,7 @@ class Protocol:
     protocol_seed: int = 1234
     recon_seed: int = 3
     fixed_partition: bool = True
+    gram_mode: int = 0
 
     @property
     def nq(self) -> int:
@@ -53,7 +54,8 @@ class Protocol:
     def params(self, lam: float = 0.0) -> ReconParams:
         return ReconParams(vol_size=tuple(self.vol), nq=self.nq, block_size=tuple(self.block),
                            prox_mode=LLR_PROX_SOFT_THRESH, lam=lam, seed=self.recon_seed,
-                           max_rand_shift=(1, 1, 1) if self.fixed_partition else None)
+                           max_rand_shift=(1, 1, 1) if self.fixed_partition else None,
+                           gram_mode=self.gram_mode)
 
     def subject(self, seed: int):
         return make_dataset(self.vol, self.shells, self.accel, seed, centre=self.centre,
@@ -64,8 +66,9 @@ def nrmse(x: np.ndarray, ref: np.ndarray) -> float:
     return float(np.linalg.norm((x - ref).ravel()) / np.linalg.norm(ref.ravel()))
 
 
-def reference(proto: Protocol, y: np.ndarray, n_iter: int):
-    """Zero-filled image, lambda = lam_rel * sigma_max of it, and the plain recon after n_iter."""
+def reference(proto: Protocol, y: np.ndarray, n_iter: int, snapshot: bool = False):
+    """Zero-filled image, lambda = lam_rel * sigma_max of it, the plain recon after n_iter and the
+    measured k-space energy; with ``snapshot`` also a device copy of the final iterate."""
     with ReconContext(proto.params()) as ctx:
         ctx.upload_kspace(y)
         ctx.init_zero_filled()
@@ -74,6 +77,8 @@ def reference(proto: Protocol, y: np.ndarray, n_iter: int):
         ctx.set_lambda(lam)
         ctx.iterate(n_iter)
         energy = ctx.measurement_stats()[0]
+        if snapshot:
+            return x_zf, ctx.download_image(), lam, energy, ctx.snapshot()
         return x_zf, ctx.download_image(), lam, energy
 
 
@@ -160,9 +165,11 @@ def warm_start_image(net: Cnn, codec: SubspaceCodec, x_zf: np.ndarray, energy: f
     return x0, ms
 
 
-def time_to_targets(proto: Protocol, y: np.ndarray, lam: float, x_start: np.ndarray, x_ref: np.ndarray,
+def time_to_targets(proto: Protocol, y: np.ndarray, lam: float, x_start: np.ndarray, snap,
                     targets: Sequence[float], max_iter: int, chunk: int = 10):
-    """For each target t: (iterations, device ms) until nrmse(x_k, x_ref) <= t, or None."""
+    """For each target t: (iterations, device ms) until the relative RMS distance of the iterate
+    to the reference snapshot (ReconContext.snapshot of the converged run) is <= t, or None.
+    The distance is taken on the device between chunks of ``chunk`` timed iterations."""
     res = {t: None for t in targets}
     curve = []
     with ReconContext(proto.params(lam)) as ctx:
@@ -170,7 +177,7 @@ def time_to_targets(proto: Protocol, y: np.ndarray, lam: float, x_start: np.ndar
         ctx.upload_image(x_start)
         ctx.iteration = 0
         it, ms = 0, 0.0
-        e = nrmse(ctx.download_image(), x_ref)
+        e = ctx.nrmse(snap)
         curve.append((0, e))
         for t in targets:
             if e <= t:
@@ -178,9 +185,53 @@ def time_to_targets(proto: Protocol, y: np.ndarray, lam: float, x_start: np.ndar
         while it < max_iter and any(v is None for v in res.values()):
             ms += ctx.iterate_timed(chunk)
             it += chunk
-            e = nrmse(ctx.download_image(), x_ref)
+            e = ctx.nrmse(snap)
             curve.append((it, e))
             for t in targets:
                 if res[t] is None and e <= t:
                     res[t] = (it, ms)
     return res, curve
+
+
+def default_weights_path() -> str:
+    import os
+    return os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "warm_start_net.npz")
+
+
+def main(argv=None) -> None:
+    """python -m llr_b200.warmstart train: builds adjoint -> converged pairs with the plain
+    recon and trains the network on the GPU; writes the parameters and the protocol."""
+    import argparse
+    import json
+    import time
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("cmd", choices=["train"])
+    ap.add_argument("--out", default=default_weights_path())
+    ap.add_argument("--vol", type=int, nargs=3, default=[96, 96, 48])
+    ap.add_argument("--centre", type=int, default=8)
+    ap.add_argument("--subjects", type=int, default=32)
+    ap.add_argument("--n-ref", type=int, default=600)
+    ap.add_argument("--epochs", type=int, default=40)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--seed", type=int, default=5)
+    a = ap.parse_args(argv)
+    proto = Protocol(vol=tuple(a.vol), centre=a.centre)
+    codec = SubspaceCodec(proto)
+    t0 = time.time()
+    pairs = training_pairs(proto, codec, list(range(1000, 1000 + a.subjects)), a.n_ref)
+    t1 = time.time()
+    net = Cnn(seed=a.seed)
+    losses = train(net, pairs, a.epochs, a.lr)
+    t2 = time.time()
+    import os
+    os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
+    info = dict(vol=list(proto.vol), centre=proto.centre, subjects=a.subjects, n_ref=a.n_ref, epochs=a.epochs,
+                lr=a.lr, seed=a.seed, protocol_seed=proto.protocol_seed, srank=proto.srank,
+                loss_first=losses[0], loss_last=losses[-1], pairs_s=round(t1 - t0, 1), train_s=round(t2 - t1, 1))
+    np.savez(a.out, channels=np.asarray(net.channels, dtype=np.int32), params=net.params,
+             info=np.asarray(json.dumps(info)))
+    print(json.dumps(info))
+
+
+if __name__ == "__main__":
+    main()

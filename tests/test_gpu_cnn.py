@@ -117,8 +117,8 @@ def test_adam_training_reduces_loss(gpu):
 def test_learned_warm_start_gain(gpu):
     """Train on the GPU (own kernels) on adjoint -> converged pairs of 16 subjects that share
     one protocol, then start a held-out subject's recon from the network's image: it starts
-    closer to the converged image than the zero-filled start and needs no more iterations to
-    reach NRMSE <= 3e-3 (the fixed-partition iteration; plain and learned share it)."""
+    closer to the converged image than the zero-filled start, needs no more iterations to reach
+    NRMSE <= 3e-2 and is no farther after 200 iterations (fixed partition, shared by both)."""
     from llr_b200 import warmstart as W
     from llr_b200.cnn import Cnn
     proto = W.Protocol(vol=(32, 32, 32), centre=8)
@@ -128,11 +128,13 @@ def test_learned_warm_start_gain(gpu):
         losses = W.train(net, pairs, epochs=30, lr=1e-3)
         assert losses[-1] < 0.8 * losses[0]
         d = proto.subject(977)
-        x_zf, x_ref, lam, energy = W.reference(proto, d.y, 1600)
+        x_zf, x_ref, lam, energy, snap = W.reference(proto, d.y, 1600, snapshot=True)
         x0, ms = W.warm_start_image(net, codec, x_zf, energy)
     e_zf, e_ws = W.nrmse(x_zf, x_ref), W.nrmse(x0, x_ref)
     assert e_ws < e_zf, (e_ws, e_zf)
-    plain, _ = W.time_to_targets(proto, d.y, lam, x_zf, x_ref, [3e-3], 800)
-    learned, _ = W.time_to_targets(proto, d.y, lam, x0, x_ref, [3e-3], 800)
-    assert plain[3e-3] is not None and learned[3e-3] is not None
-    assert learned[3e-3][0] <= plain[3e-3][0], (learned, plain)
+    plain, cp = W.time_to_targets(proto, d.y, lam, x_zf, snap, [3e-2, 1e-9], 200)
+    learned, cl = W.time_to_targets(proto, d.y, lam, x0, snap, [3e-2, 1e-9], 200)
+    assert abs(cp[0][1] - e_zf) < 1e-4 and abs(cl[0][1] - e_ws) < 1e-4   # device distance = host NRMSE
+    assert plain[3e-2] is not None and learned[3e-2] is not None
+    assert learned[3e-2][0] <= plain[3e-2][0], (learned, plain)
+    assert cl[-1][1] <= cp[-1][1] * 1.05, (cl[-1], cp[-1])      # still at least as close after 200
