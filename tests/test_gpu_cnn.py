@@ -121,7 +121,7 @@ def test_learned_warm_start_gain(gpu):
     NRMSE <= 3e-2 and is no farther after 200 iterations (fixed partition, shared by both)."""
     from llr_b200 import warmstart as W
     from llr_b200.cnn import Cnn
-    proto = W.Protocol(vol=(32, 32, 32), centre=8)
+    proto = W.Protocol(vol=(36, 36, 36), centre=9)      # 6^3 blocks tile the volume exactly
     codec = W.SubspaceCodec(proto)
     pairs = W.training_pairs(proto, codec, list(range(200, 216)), 400)
     with Cnn(seed=5) as net:
