@@ -9,13 +9,16 @@
 //
 // A warp owns one block at a time and synchronises only with __syncwarp, so blocks of very
 // different cost (all-zero, certified-zero, full eigen path) never wait on each other:
-//   * soft threshold, ||G||_F <= lambda^2: every eigenvalue is below lambda^2 -> r_a = 0;
-//   * soft threshold, max_i G_ii > lambda^2: the top eigenvalue is above -> eigen path;
-//   * otherwise a Cholesky factorisation of lambda^2 I - G certifies r_a = 0 when it
-//     succeeds (every pivot positive) and sends the block to the eigen path when it fails;
+//   (tau = (1 - margin) lambda^2 below; eigenvalues between tau and lambda^2 are near threshold)
+//   * soft threshold, ||G||_F <= tau: every eigenvalue is clear below the threshold -> r_a = 0;
+//   * soft threshold, max_i G_ii > tau: the top eigenvalue is kept or near -> eigen path;
+//   * otherwise a Cholesky factorisation of tau I - G certifies r_a = 0 when it succeeds
+//     (every pivot positive) and sends the block to the eigen path when it fails;
 //   * eigen path: Householder tridiagonalisation, unitary diagonal to a real tridiagonal T',
-//     Sturm count for r_a, multisection for the kept eigenvalues, twisted-factorisation
-//     eigenvectors with Gram-Schmidt and a residual check, back-transformation V = Q D Y.
+//     Sturm counts for the kept and the near-threshold eigenvalues, multisection for them,
+//     twisted-factorisation eigenvectors with Gram-Schmidt and a residual check,
+//     back-transformation V = Q D Y.  The apply kernel recomputes every column's gain from
+//     ||C v||^2 accumulated in FP64 (the refinement sweep: no squared conditioning).
 // Blocks keeping more than kFacCols components, or whose eigenvectors fail the residual
 // check, get r_a = -1 and go to the Jacobi kernel; hard rank >= n leaves the block as is
 // (r_a = -2).
@@ -29,6 +32,10 @@ namespace llr {
 namespace {
 
 constexpr int kEigWarps = 2;   // warps (independent blocks) per CTA
+// Eigenvalues within this relative margin below lambda^2 are kept as factor columns too (gain
+// 0 in FP32): the apply kernel refines every column's singular value from ||C v||^2 with FP64
+// accumulation, where FP32 Gram eigenvalues carry an absolute error ~ eps * sigma_1^2.
+constexpr float kRefineMargin = 0.1f;
 
 template <int NPMAX>
 struct WarpEig {
@@ -435,6 +442,7 @@ __global__ void __launch_bounds__(32 * kEigWarps) llr_eig_warp_kernel(ProxOp op,
   const int P = n * (n + 1) / 2;
   const bool soft = op.mode != LLR_PROX_HARD_RANK;
   const float thr = op.lambda * op.lambda;
+  const float thr_lo = thr * (1.f - kRefineMargin);
   int* counter = op.blk_ra + nblocks;   // dynamic block queue, zeroed before the launch
   for (;;) {
     int bi = 0;
@@ -462,12 +470,12 @@ __global__ void __launch_bounds__(32 * kEigWarps) llr_eig_warp_kernel(ProxOp op,
       ra = -2;                                            // identity: leave the block as is
     } else if (soft && !(op.lambda > 0.f)) {
       ra = -2;                                            // no threshold: identity
-    } else if (soft && fro2 <= thr * thr) {
-      ra = 0;                                             // lambda_max <= ||G||_F <= lambda^2
+    } else if (soft && fro2 <= thr_lo * thr_lo) {
+      ra = 0;                                             // lambda_max <= ||G||_F, clear of the margin
     } else {
-      bool eig = !soft || dmax > thr;                     // lambda_max >= max_i G_ii
+      bool eig = !soft || dmax > thr_lo;                  // lambda_max >= max_i G_ii
       if (!eig) {
-        eig = !warp_below(W, n, thr);
+        eig = !warp_below(W, n, thr_lo);
         if (eig) {                                        // the test overwrote A: reload
           for (int i = lane; i < P; i += 32) W->A[i] = G[i];
           __syncwarp();
@@ -478,14 +486,21 @@ __global__ void __launch_bounds__(32 * kEigWarps) llr_eig_warp_kernel(ProxOp op,
       } else {
         warp_tridiag(W, n);
         const TriInfo ti = warp_setup(W, n);
-        int nb;
-        if (!soft) nb = n - op.rank;
-        else nb = sturm_below(W->d, W->e2, n, thr, ti.pivmin);   // every lane, same answer
-        ra = n - nb;
+        int nb, nb_lo;
+        if (!soft) {
+          nb = nb_lo = n - op.rank;
+        } else {                                          // every lane runs the count: same answer
+          nb = sturm_below(W->d, W->e2, n, thr, ti.pivmin);
+          nb_lo = sturm_below(W->d, W->e2, n, thr_lo, ti.pivmin);
+        }
+        ra = n - nb;                                      // kept in FP32
         if (ra > kFacCols) {
           ra = -1;
-        } else if (ra > 0) {
-          warp_eigenvalues(W, n, nb, ra, ti);
+        } else {
+          ra = min(n - nb_lo, kFacCols);                  // plus the near-threshold ones
+        }
+        if (ra > 0) {
+          warp_eigenvalues(W, n, n - ra, ra, ti);
           if (!warp_vectors(W, n, ra, ti)) {
             ra = -1;
           } else {

@@ -904,13 +904,85 @@ __global__ void __launch_bounds__(kEigThreads, 4) llr_eig_apply_kernel(BlockSour
   }
 }
 
+// Soft-threshold apply with the refinement sweep: t_a = C v_a for the thread's (at most two)
+// rows, sigma_a^2 = ||C v_a||^2 / ||v_a||^2 summed over the block in FP64 (no Gram: the
+// conditioning is not squared), g_a = max(1 - lambda / sigma_a, 0), then C' = sum_a t_a g_a v_a^H.
+template <int RM>
+__device__ void apply_rows_refined(const BlockSource& s, long long base, const RowTab* rows, const float2* rowph,
+                                   int m, int n, long long qstride, const float2* Va, float* g, int ra, float lam,
+                                   double* red) {
+  constexpr int KB = 8;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  float2 t[2][RM];
+  double mu[RM];
+#pragma unroll
+  for (int a = 0; a < RM; ++a) mu[a] = 0.0;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int r = tid + h * blockDim.x;
+#pragma unroll
+    for (int a = 0; a < RM; ++a) t[h][a] = make_float2(0.f, 0.f);
+    if (r < m) {
+      const RowTab rt = rows[r];
+      for (int k0 = 0; k0 < n; k0 += KB) {
+        float2 c[KB];
+#pragma unroll
+        for (int u = 0; u < KB; ++u)
+          c[u] = (k0 + u < n) ? load_elem(s, base, rt, rowph, r, k0 + u, qstride) : make_float2(0.f, 0.f);
+#pragma unroll
+        for (int u = 0; u < KB; ++u) {
+          if (k0 + u < n) {
+#pragma unroll
+            for (int a = 0; a < RM; ++a)
+              if (a < ra) cfma(t[h][a], c[u], Va[(k0 + u) * kFacCols + a]);
+          }
+        }
+      }
+#pragma unroll
+      for (int a = 0; a < RM; ++a) mu[a] += (double)t[h][a].x * t[h][a].x + (double)t[h][a].y * t[h][a].y;
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < RM; ++a) {
+    for (int o = 16; o > 0; o >>= 1) mu[a] += __shfl_xor_sync(0xffffffffu, mu[a], o);
+    if (lane == 0) red[warp * RM + a] = mu[a];
+  }
+  __syncthreads();
+  if (tid < ra) {
+    double sum = 0.0, vn = 0.0;
+    for (int w = 0; w < nw; ++w) sum += red[w * RM + tid];
+    for (int q = 0; q < n; ++q) {
+      const float2 v = Va[q * kFacCols + tid];
+      vn += (double)v.x * v.x + (double)v.y * v.y;
+    }
+    const double sig = vn > 0.0 ? sqrt(sum / vn) : 0.0;
+    g[tid] = sig > (double)lam ? (float)(1.0 - (double)lam / sig) : 0.f;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int r = tid + h * blockDim.x;
+    if (r >= m) continue;
+    const RowTab rt = rows[r];
+#pragma unroll
+    for (int a = 0; a < RM; ++a) t[h][a] = cscale(t[h][a], a < ra ? g[a] : 0.f);
+    for (int q = 0; q < n; ++q) {
+      float2 c = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int a = 0; a < RM; ++a)
+        if (a < ra) cfma_cb(c, t[h][a], Va[q * kFacCols + a]);
+      store_elem(s, base, rt, rowph, r, q, qstride, c);
+    }
+  }
+}
+
 // C' = (C V_a) diag(g) V_a^H for the blocks whose eigen factor the warp eigen kernel wrote
 // (r_a > 0), zero for r_a = 0; r_a = -1 (Jacobi fallback) and -2 (identity) are left alone.
 // One CTA per block, one thread per row with eight loads in flight.
 constexpr int kApplyThreads = 256;
 
 struct ApplyLayout {
-  size_t off_row, off_rowph, off_V, off_g, total;
+  size_t off_row, off_rowph, off_V, off_g, off_red, total;
 };
 
 inline ApplyLayout make_apply_layout(int m, int n) {
@@ -920,6 +992,7 @@ inline ApplyLayout make_apply_layout(int m, int n) {
   L.off_rowph = off; off = align16(off + sizeof(float2) * (size_t)m);
   L.off_V = off; off = align16(off + sizeof(float2) * (size_t)n * kFacCols);
   L.off_g = off; off = align16(off + sizeof(float) * kFacCols);
+  L.off_red = off; off = align16(off + sizeof(double) * (kApplyThreads / 32) * kFacCols);
   L.total = off;
   return L;
 }
@@ -931,8 +1004,11 @@ __global__ void __launch_bounds__(kApplyThreads, 4) llr_apply_kernel(BlockSource
   float2* rowph = reinterpret_cast<float2*>(smem + L.off_rowph);
   float2* Va = reinterpret_cast<float2*>(smem + L.off_V);
   float* g = reinterpret_cast<float*>(smem + L.off_g);
+  double* red = reinterpret_cast<double*>(smem + L.off_red);
   const int m = op.m, n = op.n, tid = threadIdx.x;
   const long long qstride = src.kind == 1 ? src.g.V : (long long)m;
+  // soft threshold: gains from ||C v||^2 (FP64 sum) when the block's rows fit two per thread
+  const bool refine = op.mode != LLR_PROX_HARD_RANK && m <= 2 * (int)blockDim.x;
   if (tid == 0) block_shift(src, sh_s);
   __syncthreads();
   const int sh[3] = {sh_s[0], sh_s[1], sh_s[2]};
@@ -968,6 +1044,10 @@ __global__ void __launch_bounds__(kApplyThreads, 4) llr_apply_kernel(BlockSource
         const int q = idx / m, r = idx - q * m;
         store_elem(src, base, rows[r], rowph, r, q, qstride, make_float2(0.f, 0.f));
       }
+    } else if (refine) {
+      if (ra <= 2) apply_rows_refined<2>(src, base, rows, rowph, m, n, qstride, Va, g, ra, op.lambda, red);
+      else if (ra <= 4) apply_rows_refined<4>(src, base, rows, rowph, m, n, qstride, Va, g, ra, op.lambda, red);
+      else apply_rows_refined<kFacCols>(src, base, rows, rowph, m, n, qstride, Va, g, ra, op.lambda, red);
     } else if (ra <= 2) {
       apply_rows<2, kFacCols>(src, base, rows, rowph, m, n, qstride, Va, g, ra);
     } else if (ra <= 4) {

@@ -310,3 +310,27 @@ def test_hard_project_matches_reference(gpu):
     exp, e = O.hard_project(x, y)
     np.testing.assert_array_equal(got, exp)
     assert abs(err.value - e) <= 1e-6 * e
+
+
+def test_near_threshold_gains_refined(gpu):
+    """Singular values within 0.2 % of the threshold next to a dominant one (sigma_1 = 40 lambda):
+    the Gram eigenvalues carry an absolute error ~ eps sigma_1^2, the refinement sweep takes the
+    gains from ||C v||^2 with FP64 accumulation.  The output restricted to the near-threshold
+    singular vectors must match the FP64 oracle to 1e-4 lambda."""
+    rng = np.random.default_rng(31)
+    m, n, lam = 216, 61, 1.0
+    sig = []
+    for k in range(12):
+        s = [40.0, 1.0 + 2e-3, 1.0 - 2e-3, 1.0 + 5e-4] + list(rng.uniform(0.05, 0.6, n - 4))
+        sig.append(s)
+    A = _spectrum_blocks(rng, m, n, sig).astype(np.complex64)
+    d = DeviceBuffer.from_array(A)
+    L.check(L.lib.llr_soft_threshold_batch_dev(m, n, lam, A.shape[2], d.ptr, None))
+    got = d.download(np.empty_like(A, order="F")).astype(np.complex128)
+    A64 = A.astype(np.complex128)
+    exp = O.low_rank_soft(A64, lam)
+    for b in range(A.shape[2]):
+        _, s, Vh = np.linalg.svd(A64[:, :, b], full_matrices=False)
+        near = Vh[1:4].conj().T                      # right singular vectors at 1 +- 2e-3, 1 + 5e-4
+        err = np.linalg.norm((got[:, :, b] - exp[:, :, b]) @ near)
+        assert err < 1e-4 * lam, (b, err, s[:4])
