@@ -259,6 +259,19 @@ int llr_memcpy_d2h(void* dst, const void* src, size_t bytes, void* stream);
 int llr_stream_sync(void* stream);
 int llr_device_count(int32_t* n);
 
+/* ---- data-set files (host only, no GPU) --------------------------------------------
+ * CFL volumes as the reference's dataset builder and writer use them (data_import.rs:67-108,
+ * lib.rs:353-362, the cfl crate's format): <name>.hdr ("# Dimensions" and the sizes, first
+ * fastest) and <name>.cfl (raw complex64, column-major).  A ".cfl"/".hdr" suffix on the path is
+ * ignored.  The b-table reader takes four numbers per volume, b-value and gradient vector
+ * (data_import.rs:110-145; ".txt" is appended when the path has no extension); the b0 mask
+ * marks gradient vectors of norm <= tol (data_import.rs:322-328). */
+int llr_cfl_dims(const char* path, int64_t* dims, int32_t max_dims, int32_t* ndims);
+int llr_cfl_read(const char* path, llr_cf32* dst, int64_t count);
+int llr_cfl_write(const char* path, const int64_t* dims, int32_t ndims, const llr_cf32* src);
+int llr_read_b_table(const char* path, int32_t n_vols, float* b_vals, float* b_vecs);
+int llr_b0_mask(const float* b_vecs, int32_t n_vols, float tol, uint8_t* is_b0);
+
 /* ---- learned warm start: 3-D residual CNN ----------------------------------------
  * No reference counterpart: the reference has no learned component.  A network of
  * n_layers conv3d 3x3x3 layers (zero padding, ReLU between layers, out = in + net(in));

@@ -146,6 +146,11 @@ SIGNATURES = {
     "llr_memcpy_d2h": (C.c_int, [P, P, SZ, P]),
     "llr_stream_sync": (C.c_int, [P]),
     "llr_device_count": (C.c_int, [PI32]),
+    "llr_cfl_dims": (C.c_int, [C.c_char_p, C.POINTER(I64), I32, PI32]),
+    "llr_cfl_read": (C.c_int, [C.c_char_p, P, I64]),
+    "llr_cfl_write": (C.c_int, [C.c_char_p, C.POINTER(I64), I32, P]),
+    "llr_read_b_table": (C.c_int, [C.c_char_p, I32, PF32, PF32]),
+    "llr_b0_mask": (C.c_int, [PF32, I32, C.c_float, P]),
     "llr_cnn_create": (C.c_int, [I32, PI32, I32, U64, C.POINTER(P)]),
     "llr_cnn_destroy": (C.c_int, [P]),
     "llr_cnn_param_count": (C.c_int, [P, C.POINTER(I64)]),
