@@ -272,6 +272,16 @@ int llr_cfl_write(const char* path, const int64_t* dims, int32_t ndims, const ll
 int llr_read_b_table(const char* path, int32_t n_vols, float* b_vals, float* b_vecs);
 int llr_b0_mask(const float* b_vecs, int32_t n_vols, float tol, uint8_t* is_b0);
 
+/* ---- DTI scalar maps (diffusion_models.rs:21-129, calc_scalars) --------------------
+ * Per voxel: s0 = mean |b0|, ln-signal ratios clamped as build_rhs, the least-squares tensor
+ * of build_design_matrix's columns, its eigenvalues e1 >= e2 >= e3, MD, RD, FA.  Volumes are
+ * (n_vox) complex64 each, volume-major; out receives 7 planes of n_vox floats: b0av, e1, e2,
+ * e3, md, rd, fa.  nq >= 6 diffusion-weighted volumes with b_vals (nq), b_vecs (nq x 3). */
+int llr_dti_fit_dev(const llr_cf32* d_dwi, int32_t nq, const llr_cf32* d_b0, int32_t nb0, int64_t n_vox,
+                    const float* b_vals, const float* b_vecs, float* d_out, void* stream);
+int llr_dti_fit(const llr_cf32* dwi, int32_t nq, const llr_cf32* b0, int32_t nb0, int64_t n_vox,
+                const float* b_vals, const float* b_vecs, float* out);
+
 /* ---- learned warm start: 3-D residual CNN ----------------------------------------
  * No reference counterpart: the reference has no learned component.  A network of
  * n_layers conv3d 3x3x3 layers (zero padding, ReLU between layers, out = in + net(in));

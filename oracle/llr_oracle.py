@@ -693,3 +693,44 @@ def sigma_max(x: np.ndarray, block_size, shift=(0, 0, 0)) -> float:
 def nrmse(x: np.ndarray, ref: np.ndarray) -> float:
     """||x - ref||_2 / ||ref||_2 over all volumes."""
     return float(np.linalg.norm((x - ref).ravel()) / np.linalg.norm(ref.ravel()))
+
+
+# ---------------------------------------------------------------------------------------
+# DTI scalar maps (diffusion_models.rs:21-129)
+# ---------------------------------------------------------------------------------------
+def dti_design_matrix(b: np.ndarray, g: np.ndarray) -> np.ndarray:
+    """build_design_matrix (diffusion_models.rs:219-253): (nq, 6), columns -b gx^2, -b gy^2,
+    -b gz^2, -2 b gx gy, -2 b gx gz, -2 b gy gz."""
+    b = np.asarray(b, dtype=np.float64)
+    g = np.asarray(g, dtype=np.float64)
+    return np.stack([-b * g[:, 0] ** 2, -b * g[:, 1] ** 2, -b * g[:, 2] ** 2, -2 * b * g[:, 0] * g[:, 1],
+                     -2 * b * g[:, 0] * g[:, 2], -2 * b * g[:, 1] * g[:, 2]], axis=1)
+
+
+def tensor_eigenvalues(t: np.ndarray) -> np.ndarray:
+    """solve_eigenvalues (diffusion_models.rs:160-185): t (..., 6) = Dxx Dyy Dzz Dxy Dxz Dyz;
+    returns (..., 3) descending (e1 >= e2 >= e3)."""
+    t = np.asarray(t, dtype=np.float64)
+    M = np.zeros(t.shape[:-1] + (3, 3))
+    M[..., 0, 0], M[..., 1, 1], M[..., 2, 2] = t[..., 0], t[..., 1], t[..., 2]
+    M[..., 1, 0] = M[..., 0, 1] = t[..., 3]
+    M[..., 2, 0] = M[..., 0, 2] = t[..., 4]
+    M[..., 2, 1] = M[..., 1, 2] = t[..., 5]
+    return np.linalg.eigvalsh(M)[..., ::-1]
+
+
+def dti_fit(dwi: np.ndarray, b0: np.ndarray, b: np.ndarray, g: np.ndarray) -> dict:
+    """calc_scalars (diffusion_models.rs:21-112) on (V, nq) and (V, nb0) complex arrays: b0 average
+    of magnitudes, rhs = ln(clamp(|s| / max(s0, FLT_MIN), FLT_MIN, 1)), least-squares tensor,
+    eigenvalues, MD, RD, FA."""
+    tiny = np.finfo(np.float32).tiny
+    s0 = np.abs(b0).mean(axis=1) if b0.shape[1] else np.zeros(dwi.shape[0])
+    rhs = np.log(np.clip(np.abs(dwi) / np.maximum(s0, tiny)[:, None], tiny, 1.0))
+    A = dti_design_matrix(b, g)
+    t = np.linalg.lstsq(A, rhs.T, rcond=None)[0].T
+    e = tensor_eigenvalues(t)
+    md = e.mean(axis=1)
+    rd = 0.5 * (e[:, 1] + e[:, 2])
+    with np.errstate(invalid="ignore", divide="ignore"):
+        fa = np.sqrt(1.5) * np.sqrt(((e - md[:, None]) ** 2).sum(axis=1)) / np.sqrt((e ** 2).sum(axis=1))
+    return dict(b0av=s0, e1=e[:, 0], e2=e[:, 1], e3=e[:, 2], md=md, rd=rd, fa=fa, tensor=t)

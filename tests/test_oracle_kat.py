@@ -241,3 +241,23 @@ def test_recon_residual_decreases_small():
     cfg = O.ReconConfig(block_size=(4, 4, 4), mode="hard", rank=1, seed=3)
     _, hist = O.recon(y, cfg, 6)
     assert hist[-1] < hist[0]
+
+
+def test_dti_eigenvalue_known_answer():
+    """diffusion_models.rs:148-157: tensor (2, 1.5, 1, 0, 0, 0) has eigenvalues 1, 1.5, 2."""
+    np.testing.assert_allclose(O.tensor_eigenvalues(np.array([2.0, 1.5, 1.0, 0, 0, 0])), [2.0, 1.5, 1.0])
+
+
+def test_dti_fit_recovers_noise_free_tensor():
+    """A noise-free tensor signal S0 exp(-b g^T D g) is fitted exactly (diffusion_models.rs:61-112)."""
+    from llr_b200.phantom import b_table, eigenvector_matrix, sample_unit_sphere, tensor_signal
+    rng = np.random.default_rng(2)
+    b, g = b_table([(0, 2), (1000, 15), (2000, 15)], rng)
+    R = eigenvector_matrix(sample_unit_sphere(0.3, 0.7))
+    D = R @ np.diag([1.7e-3, 0.5e-3, 0.3e-3]) @ R.T
+    s = tensor_signal(np.array([0.8]), D[None], b, g)[0]
+    dwi = s[b > 0][None].astype(np.complex128)
+    b0 = s[b == 0][None].astype(np.complex128)
+    r = O.dti_fit(dwi, b0, b[b > 0], g[b > 0])
+    np.testing.assert_allclose([r["e1"][0], r["e2"][0], r["e3"][0]], [1.7e-3, 0.5e-3, 0.3e-3], rtol=1e-9)
+    np.testing.assert_allclose(r["md"][0], 2.5e-3 / 3, rtol=1e-9)
