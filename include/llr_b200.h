@@ -271,6 +271,10 @@ int llr_cfl_read(const char* path, llr_cf32* dst, int64_t count);
 int llr_cfl_write(const char* path, const int64_t* dims, int32_t ndims, const llr_cf32* src);
 int llr_read_b_table(const char* path, int32_t n_vols, float* b_vals, float* b_vecs);
 int llr_b0_mask(const float* b_vecs, int32_t n_vols, float tol, uint8_t* is_b0);
+/* read_affine_translation (signal_model.rs:119-176): the first line holding "Parameters:" must
+ * carry 12 numbers (a 3 x 4 affine, translation last); translation = entries 9..11 * multiplier.
+ * Translations feed the image-space linear corrections (llr_set_linear_corrections). */
+int llr_read_affine_translation(const char* path, float multiplier, float* translation);
 
 /* ---- DTI scalar maps (diffusion_models.rs:21-129, calc_scalars) --------------------
  * Per voxel: s0 = mean |b0|, ln-signal ratios clamped as build_rhs, the least-squares tensor

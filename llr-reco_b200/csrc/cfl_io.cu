@@ -5,6 +5,7 @@
 // whitespace-separated sizes (column-major, first fastest), and <name>.cfl, raw little-endian
 // complex64 (interleaved FP32 re, im) in that column-major order.  A b-table is whitespace-
 // separated numbers, four per volume: b-value, gx, gy, gz (data_import.rs:110-145).
+#include <cctype>
 #include <cerrno>
 #include <cmath>
 #include <cstdio>
@@ -135,6 +136,40 @@ int llr_read_b_table(const char* path, int32_t n_vols, float* b_vals, float* b_v
     b_vals[i] = v[4 * i];
     for (int a = 0; a < 3; ++a) b_vecs[3 * i + a] = v[4 * i + 1 + a];
   }
+  return LLR_OK;
+}
+
+int llr_read_affine_translation(const char* path, float multiplier, float* translation) {
+  if (!path || !translation) return set_error(LLR_ERR_INVALID, "null pointer");
+  FILE* f = std::fopen(path, "r");
+  if (!f) return set_error(LLR_ERR_INVALID, "failed to open %s: %s", path, std::strerror(errno));
+  std::string line;
+  char buf[4096];
+  bool found = false;
+  std::vector<float> v;
+  while (!found && std::fgets(buf, sizeof buf, f)) {
+    line = buf;
+    if (line.find("Parameters:") == std::string::npos) continue;
+    found = true;
+    // every whitespace-separated token that parses completely as a number
+    size_t i = 0;
+    while (i < line.size()) {
+      while (i < line.size() && std::isspace((unsigned char)line[i])) ++i;
+      size_t j = i;
+      while (j < line.size() && !std::isspace((unsigned char)line[j])) ++j;
+      if (j > i) {
+        const std::string tok = line.substr(i, j - i);
+        char* end = nullptr;
+        const float x = std::strtof(tok.c_str(), &end);
+        if (end && *end == '\0') v.push_back(x);
+      }
+      i = j;
+    }
+  }
+  std::fclose(f);
+  if (!found) return set_error(LLR_ERR_INVALID, "failed to find Parameter field in affine file %s", path);
+  if (v.size() != 12) return set_error(LLR_ERR_INVALID, "expected 12 matrix entries in %s, read %zu", path, v.size());
+  for (int a = 0; a < 3; ++a) translation[a] = v[9 + a] * multiplier;   // signal_model.rs:148-176
   return LLR_OK;
 }
 

@@ -43,3 +43,15 @@ def b0_mask(g: np.ndarray, tol: float = 0.0) -> np.ndarray:
     out = np.empty(g.shape[0], dtype=np.uint8)
     check(lib.llr_b0_mask(L.fptr(g), int(g.shape[0]), float(tol), L.ptr(out)))
     return out.astype(bool)
+
+
+def read_affine_translation(path: str, multiplier: float = 1.0) -> np.ndarray:
+    """Translation (3,) of an affine transform file, times ``multiplier``."""
+    out = np.empty(3, dtype=np.float32)
+    check(lib.llr_read_affine_translation(str(path).encode(), float(multiplier), L.fptr(out)))
+    return out
+
+
+def read_affine_translations(paths, multiplier: float = 1.0) -> np.ndarray:
+    """(n, 3) translations, e.g. per-volume image-space corrections for set_linear_corrections."""
+    return np.stack([read_affine_translation(p, multiplier) for p in paths])

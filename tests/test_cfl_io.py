@@ -83,3 +83,23 @@ def test_cli_reports_bad_inputs(tmp_path):
     r = subprocess.run([exe, str(tmp_path / "p"), str(tmp_path), "vol*", str(tmp_path), "out", "bt"],
                        capture_output=True, text=True)
     assert r.returncode == 1 and "no files found" in r.stderr
+
+
+def test_affine_translation_reader(tmp_path):
+    """read_affine_translation (signal_model.rs:119-176): translation = entries 9..11 of the first
+    "Parameters:" line, times the multiplier."""
+    from llr_b200 import LlrError
+    from llr_b200.cfl import read_affine_translations
+    p = tmp_path / "a0.txt"
+    p.write_text("#Insight Transform File V1.0\n#Transform 0\nTransform: AffineTransform_double_3_3\n"
+                 "Parameters: 1 0 0 0 1 0 0 0 1 1.5 -2 0.25\nFixedParameters: 0 0 0\n")
+    q = tmp_path / "a1.txt"
+    q.write_text("Parameters: 0.9 0.1 0 -0.1 0.9 0 0 0 1 3 4 5\nParameters: 9 9 9 9 9 9 9 9 9 9 9 9\n")
+    t = read_affine_translations([p, q], 2.0)
+    np.testing.assert_allclose(t, [[3.0, -4.0, 0.5], [6.0, 8.0, 10.0]])
+    (tmp_path / "bad.txt").write_text("Parameters: 1 2 3\n")
+    with pytest.raises(LlrError):
+        read_affine_translations([tmp_path / "bad.txt"])
+    (tmp_path / "none.txt").write_text("FixedParameters: 0 0 0\n")
+    with pytest.raises(LlrError):
+        read_affine_translations([tmp_path / "none.txt"])
