@@ -286,6 +286,16 @@ int llr_dti_fit_dev(const llr_cf32* d_dwi, int32_t nq, const llr_cf32* d_b0, int
 int llr_dti_fit(const llr_cf32* dwi, int32_t nq, const llr_cf32* b0, int32_t nb0, int64_t n_vox,
                 const float* b_vals, const float* b_vecs, float* out);
 
+/* ---- temporal subspace built on the GPU (no reference counterpart: the reference only
+ * loads one, lib.rs:212-222) -------------------------------------------------------------
+ * n_signals simulated tensor signals exp(-b g^T D g) (eigenvalues uniform in [lam_lo, lam_hi],
+ * principal direction uniform on the sphere, frame as eigenvector_matrix, dti_subspace.rs:13-76)
+ * from counter-based draws keyed by seed; FP64 Gram matrix on the GPU, FP64 Jacobi eigenvectors.
+ * S_out: nq x rank column-major (largest-magnitude entry of each column positive), sv_out: the
+ * rank singular values of the nq x n_signals signal matrix.  nq <= 64. */
+int llr_dti_subspace(const float* b_vals, const float* b_vecs, int32_t nq, int32_t rank, int64_t n_signals,
+                     uint64_t seed, float lam_lo, float lam_hi, llr_cf32* S_out, double* sv_out);
+
 /* ---- learned warm start: 3-D residual CNN ----------------------------------------
  * No reference counterpart: the reference has no learned component.  A network of
  * n_layers conv3d 3x3x3 layers (zero padding, ReLU between layers, out = in + net(in));

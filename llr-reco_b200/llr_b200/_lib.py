@@ -153,6 +153,7 @@ SIGNATURES = {
     "llr_b0_mask": (C.c_int, [PF32, I32, C.c_float, P]),
     "llr_read_affine_translation": (C.c_int, [C.c_char_p, C.c_float, PF32]),
     "llr_dti_fit_dev": (C.c_int, [P, I32, P, I32, I64, PF32, PF32, P, P]),
+    "llr_dti_subspace": (C.c_int, [PF32, PF32, I32, I32, I64, U64, C.c_float, C.c_float, P, PF64]),
     "llr_dti_fit": (C.c_int, [P, I32, P, I32, I64, PF32, PF32, PF32]),
     "llr_cnn_create": (C.c_int, [I32, PI32, I32, U64, C.POINTER(P)]),
     "llr_cnn_destroy": (C.c_int, [P]),

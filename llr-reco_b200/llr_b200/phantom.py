@@ -175,3 +175,19 @@ def dti_subspace(b: np.ndarray, g: np.ndarray, rank: int, n_signals: int, seed: 
     sig = tensor_signal(np.ones(n_signals), D, b, g)     # (n, nq)
     U, s, _ = np.linalg.svd(sig.T, full_matrices=False)
     return np.asfortranarray(U[:, :rank].astype(np.complex64))
+
+
+def dti_subspace_gpu(b: np.ndarray, g: np.ndarray, rank: int, n_signals: int, seed: int,
+                     lam_lo: float = 0.1e-3, lam_hi: float = 3.0e-3):
+    """The same subspace construction on the GPU (llr_dti_subspace, counter-based draws):
+    returns (S (nq, rank) complex64, singular values)."""
+    import ctypes as C
+    from . import _lib as L
+    nq = len(b)
+    bb = np.ascontiguousarray(b, dtype=np.float32)
+    gg = np.ascontiguousarray(g, dtype=np.float32)
+    S = np.empty((nq, rank), dtype=np.complex64, order="F")
+    sv = np.empty(rank, dtype=np.float64)
+    L.check(L.lib.llr_dti_subspace(L.fptr(bb), L.fptr(gg), nq, rank, int(n_signals), C.c_uint64(seed),
+                                   float(lam_lo), float(lam_hi), L.ptr(S), sv.ctypes.data_as(L.PF64)))
+    return S, sv

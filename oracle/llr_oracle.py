@@ -734,3 +734,51 @@ def dti_fit(dwi: np.ndarray, b0: np.ndarray, b: np.ndarray, g: np.ndarray) -> di
     with np.errstate(invalid="ignore", divide="ignore"):
         fa = np.sqrt(1.5) * np.sqrt(((e - md[:, None]) ** 2).sum(axis=1)) / np.sqrt((e ** 2).sum(axis=1))
     return dict(b0av=s0, e1=e[:, 0], e2=e[:, 1], e3=e[:, 2], md=md, rd=rd, fa=fa, tensor=t)
+
+
+# ---------------------------------------------------------------------------------------
+# Temporal subspace from simulated tensor signals (the library's GPU construction)
+# ---------------------------------------------------------------------------------------
+SUBSPACE_STREAM = 0x5342  # "SB"
+
+
+def _rng_u64_vec(seed: int, stream: int, index: np.ndarray) -> np.ndarray:
+    """rng_u64 over an array of indices (uint64 arithmetic wraps modulo 2^64)."""
+    with np.errstate(over="ignore"):
+        g = np.uint64(GOLDEN64)
+        x = np.uint64(seed) + g * ((np.uint64(stream) << np.uint64(32)) + index.astype(np.uint64) + np.uint64(1))
+        z = x + g
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return z ^ (z >> np.uint64(31))
+
+
+def dti_subspace_counter(b, g, rank: int, n_signals: int, seed: int, lam_lo=0.1e-3, lam_hi=3.0e-3):
+    """Leading left singular vectors of n_signals simulated tensor signals (S0 = 1), drawn with the
+    counter RNG: direction (sample_unit_sphere, dti_subspace.rs:65-76) from draws 5i, 5i+1,
+    eigenvalues uniform in [lam_lo, lam_hi] from draws 5i+2..5i+4, frame as eigenvector_matrix
+    (dti_subspace.rs:13-44).  Returns (S (nq, rank) with the largest-magnitude entry of each column
+    positive, singular values (rank,))."""
+    b = np.asarray(b, dtype=np.float64)
+    g = np.asarray(g, dtype=np.float64)
+    i = np.arange(n_signals, dtype=np.uint64)
+    u = [((_rng_u64_vec(seed, SUBSPACE_STREAM, 5 * i + k) >> np.uint64(11)).astype(np.float64) + 0.5) / 2.0 ** 53
+         for k in range(5)]
+    th, ph = 2 * np.pi * u[0], np.arccos(2 * u[1] - 1)
+    e1 = np.stack([np.sin(ph) * np.cos(th), np.sin(ph) * np.sin(th), np.cos(ph)], axis=1)
+    e1 /= np.linalg.norm(e1, axis=1, keepdims=True)
+    near_x = np.abs(e1[:, 0] - 1.0) < np.finfo(np.float32).eps
+    tmp = np.where(near_x[:, None], [0.0, 1.0, 0.0], [1.0, 0.0, 0.0])
+    e2 = np.cross(e1, tmp)
+    e2 /= np.linalg.norm(e2, axis=1, keepdims=True)
+    e3 = np.cross(e1, e2)
+    lam = np.stack([lam_lo + (lam_hi - lam_lo) * u[k] for k in (2, 3, 4)], axis=1)
+    proj = np.stack([e1 @ g.T, e2 @ g.T, e3 @ g.T], axis=2)          # (n, nq, 3)
+    sig = np.exp(-b[None, :] * np.einsum("nqa,na->nq", proj ** 2, lam))
+    G = sig.T @ sig
+    w, V = np.linalg.eigh(G)
+    order = np.argsort(w)[::-1][:rank]
+    S = V[:, order]
+    idx = np.argmax(np.abs(S), axis=0)
+    S = S * np.sign(S[idx, np.arange(rank)])
+    return S.astype(np.complex128), np.sqrt(np.maximum(w[order], 0.0))

@@ -334,3 +334,18 @@ def test_near_threshold_gains_refined(gpu):
         near = Vh[1:4].conj().T                      # right singular vectors at 1 +- 2e-3, 1 + 5e-4
         err = np.linalg.norm((got[:, :, b] - exp[:, :, b]) @ near)
         assert err < 1e-4 * lam, (b, err, s[:4])
+
+
+def test_subspace_construction_matches_oracle(gpu):
+    """GPU temporal subspace (simulated signals, FP64 Gram, FP64 Jacobi) against the oracle's
+    restatement with the same counter-based draws: the same subspace and singular values."""
+    from llr_b200.phantom import b_table, dti_subspace_gpu
+    b, g = b_table([(0, 1), (1000, 30), (2000, 30)], np.random.default_rng(3))
+    S, sv = dti_subspace_gpu(b, g, 7, 20000, 5)
+    f32 = lambda v: np.float64(np.float32(v))              # the ABI takes the b-table and ranges in FP32
+    Se, sve = O.dti_subspace_counter(b.astype(np.float32), g.astype(np.float32), 7, 20000, 5, f32(0.1e-3), f32(3.0e-3))
+    np.testing.assert_allclose(sv, sve, rtol=1e-9)
+    assert np.abs(S.imag).max() == 0
+    P, Pe = S.astype(np.complex128) @ S.conj().T.astype(np.complex128), Se @ Se.conj().T
+    assert np.linalg.norm(P - Pe) < 1e-6
+    np.testing.assert_allclose(S.real, Se.real, atol=1e-6)   # same sign convention
