@@ -217,9 +217,14 @@ def warm_start_headline(args, c, d) -> dict:
 def workload_label(name: str, c: dict, nq: int) -> str:
     v = c["vol"]
     b = c["block"]
+    n = c.get("srank", nq)
+    extra = ""
+    if "srank" in c:
+        extra = (f", rank-{c['srank']} temporal subspace (LLR on coefficients), "
+                 f"{c['wavelet_levels']}-level db{c['wavelet_moments']} wavelet shrink alpha {c['wavelet_alpha']:g}")
     return (f"{name}: {v[0]}x{v[1]}x{v[2]} complex64 x {nq} volumes, {b[0]}^3 LLR blocks (Casorati "
-            f"{b[0] * b[1] * b[2]}x{nq}), {c['accel']:g}x VD line sampling, soft threshold 0.02 sigma_max, FP32, "
-            f"one proximal-gradient iteration per step")
+            f"{b[0] * b[1] * b[2]}x{n}){extra}, {c['accel']:g}x VD line sampling, soft threshold 0.02 sigma_max, "
+            f"FP32, one proximal-gradient iteration per step")
 
 
 # ---------------------------------------------------------------------------------------
@@ -238,7 +243,14 @@ def run_b200(args, dist: Dist) -> None:
     params = ReconParams(vol_size=(nx, ny, nz), nq=nq, block_size=c["block"], prox_mode=llr_b200.LLR_PROX_SOFT_THRESH,
                          lam=0.0, seed=args.seed, device=dev, gram_mode=args.gram_mode,
                          eig_solver=args.eig_solver, fft_mode=args.fft_mode)
+    if "srank" in c:   # subspace + wavelet configuration: subspace built on the GPU from the b-table
+        from llr_b200.phantom import dti_subspace_gpu
+        params.subspace_rank = c["srank"]
+        params.wavelet_alpha, params.wavelet_moments = c["wavelet_alpha"], c["wavelet_moments"]
+        params.wavelet_levels = c["wavelet_levels"]
     ctx = ReconContext(params)
+    if "srank" in c:
+        ctx.upload_subspace(dti_subspace_gpu(d.b, d.g, c["srank"], 100000, args.seed)[0])
     ctx.upload_kspace(d.y)
     ctx.init_zero_filled()
     sigma = ctx.sigma_max((0, 0, 0))
@@ -268,7 +280,9 @@ def run_b200(args, dist: Dist) -> None:
     achieved = prox_bytes / (per_launch_ms["llr_prox"] / 1e3) / 1e9
     traffic = profiled_traffic("llr_prox", args.config)
     it_bytes = 16.0 * E * 3 + 24.0 * E / c["accel"]
-    roofline = {"bound": "hbm", "kernel": "LLR prox stage: llr_gram_tc_kernel + llr_eig_apply_kernel",
+    prox_label = ("LLR prox stage: llr_subspace_kernel (X <- LR(X S) S^H)" if "srank" in c else
+                  "LLR prox stage: llr_gram_tc_kernel + llr_eig_warp_kernel + llr_apply_kernel")
+    roofline = {"bound": "hbm", "kernel": prox_label,
                 "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "peak_source": peaks["source"],
                 "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4),
                 "algorithmic_bytes_per_launch": prox_bytes, "traffic": traffic,
@@ -327,7 +341,7 @@ def run_b200(args, dist: Dist) -> None:
             "config": {"workload": workload_label(args.config, c, nq), "vol": list(c["vol"]), "nq": nq,
                        "block": list(c["block"]), "accel": c["accel"], "measured_undersampling":
                            round(ctx.measurement_stats()[1], 3), "lambda": 0.02 * sigma,
-                       "l2": "no flush: the 1.73 GB iterate exceeds the 126 MB L2", "parallelism": f"replicas x{dist.world}",
+                       "l2": f"no flush: the {8 * E / 1e9:.2f} GB iterate exceeds the 126 MB L2", "parallelism": f"replicas x{dist.world}",
                        "path": "hybrid (x-transform eliminated)"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "warm_start": headline,
             "gpu_launches": n_kernels * args.steps,
