@@ -99,13 +99,13 @@ __device__ bool warp_below(WarpEig<NPMAX>* W, int n, float thr) {
     __syncwarp();
     const int rb1 = rp.i1 >= 0 ? pk(o + rp.i1, o) : 0, rb2 = rp.i2 >= 0 ? pk(o + rp.i2, o) : 0;
     const float2 nl1 = make_float2(-l1.x, -l1.y), nl2 = make_float2(-l2.x, -l2.y);
+    float2 cl = nl1;
+    int jo = 0, ib = rb1;
     for (int t = 0; t < rp.tot; ++t) {
-      const bool first = t < rp.n1;
-      const int j = first ? t : t - rp.n1;
-      const int idx = (first ? rb1 : rb2) + j;
-      float2 a = A[idx];
-      cfma_cb(a, first ? nl1 : nl2, W->u[j]);
-      A[idx] = a;
+      if (t == rp.n1) { cl = nl2; jo = rp.n1; ib = rb2 - rp.n1; }
+      float2 a = A[ib + t];
+      cfma_cb(a, cl, W->u[t - jo]);
+      A[ib + t] = a;
     }
     __syncwarp();
   }
@@ -173,14 +173,16 @@ __device__ void warp_tridiag(WarpEig<NPMAX>* W, int n) {
     // A22 -= u w^H + w u^H on the lower triangle of the lane's rows
     const float2 nu1 = make_float2(-x1.x, -x1.y), nu2 = make_float2(-x2.x, -x2.y);
     const float2 nw1 = make_float2(-w1.x, -w1.y), nw2 = make_float2(-w2.x, -w2.y);
+    // one pass over both rows: the row switch happens once per lane, not as selects per element
+    float2 cu = nu1, cw = nw1;
+    int jo = 0, ib = rb1;
     for (int s = 0; s < rp.tot; ++s) {
-      const bool first = s < rp.n1;
-      const int j = first ? s : s - rp.n1;
-      const int idx = (first ? rb1 : rb2) + j;
-      float2 a = A[idx];
-      cfma_cb(a, first ? nu1 : nu2, W->w[j]);
-      cfma_cb(a, first ? nw1 : nw2, W->u[j]);
-      A[idx] = a;
+      if (s == rp.n1) { cu = nu2; cw = nw2; jo = rp.n1; ib = rb2 - rp.n1; }
+      const int j = s - jo;
+      float2 a = A[ib + s];
+      cfma_cb(a, cu, W->w[j]);
+      cfma_cb(a, cw, W->u[j]);
+      A[ib + s] = a;
     }
     __syncwarp();
   }
