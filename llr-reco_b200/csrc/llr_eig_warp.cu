@@ -40,13 +40,19 @@ constexpr float kRefineMargin = 0.1f;
 template <int NPMAX>
 struct WarpEig {
   float2 A[NPMAX * (NPMAX + 1) / 2];   // packed lower triangle; later Householder vectors
-  float2 u[NPMAX];                     // Householder vector / Cholesky column
-  float2 w[NPMAX];                     // p - K u
-  float2 e[NPMAX];                     // complex sub-diagonal of T
+  union {
+    struct {
+      float2 u[NPMAX];                 // Householder vector / Cholesky column
+      float2 w[NPMAX];                 // p - K u
+      float2 e[NPMAX];                 // complex sub-diagonal of T
+      float e2[NPMAX];                 // |e|^2 for the Sturm counts
+      float spare[NPMAX];
+    };
+    float um[kFacCols * NPMAX];        // eigenvector stage: D+ / U- of each lane's factorisation
+  };
   float2 delta[NPMAX];                 // unitary diagonal: T' = D^H T D real
   float d[NPMAX];
   float ae[NPMAX];
-  float e2[NPMAX];
   float tau[NPMAX];
   float lam[kFacCols];
   float Y[kFacCols * NPMAX];           // eigenvectors of T', column a at Y[a * NPMAX]
@@ -144,45 +150,68 @@ __device__ void warp_tridiag(WarpEig<NPMAX>* W, int n) {
     if (rp.i1 >= 0) W->u[rp.i1] = x1;
     if (rp.i2 >= 0) W->u[rp.i2] = x2;
     __syncwarp();
-    // p = t A22 u, reading A22[i][j] = conj(A22[j][i]) above the diagonal
-    float2 p1 = z, p2 = z;
-    const int rb1 = rp.i1 >= 0 ? pk(o + rp.i1, o) : 0, rb2 = rp.i2 >= 0 ? pk(o + rp.i2, o) : 0;
-    int cb = pk(o, o);
-    for (int j = 0; j < L; ++j) {
-      const float2 uj = W->u[j];
-      if (rp.i1 >= 0) {
-        float2 a = A[j <= rp.i1 ? rb1 + j : cb + rp.i1];
-        if (j > rp.i1) a.y = -a.y;
-        cfma(p1, a, uj);
+    // p = t A22 u, reading A22[i][j] = conj(A22[j][i]) above the diagonal.  Lanes without a
+    // row read row 0 (a valid element) and drop the result; four columns are in flight at once.
+    const int r1 = max(rp.i1, 0), r2 = max(rp.i2, 0);
+    const int rb1 = pk(o + r1, o), rb2 = pk(o + r2, o);
+    float2 p1 = z, p2 = z, q1 = z, q2 = z;
+    for (int j0 = 0; j0 < L; j0 += 4) {
+      float2 a1[4], a2[4], uj[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int j = min(j0 + e, L - 1);
+        const int cb = pk(o + j, o);              // trailing row j
+        uj[e] = W->u[j];
+        a1[e] = A[j <= r1 ? rb1 + j : cb + r1];
+        a2[e] = A[j <= r2 ? rb2 + j : cb + r2];
       }
-      if (rp.i2 >= 0) {
-        float2 a = A[j <= rp.i2 ? rb2 + j : cb + rp.i2];
-        if (j > rp.i2) a.y = -a.y;
-        cfma(p2, a, uj);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int j = j0 + e;
+        if (j < L) {                              // warp-uniform
+          float2 b1 = a1[e], b2 = a2[e];
+          if (j > r1) b1.y = -b1.y;
+          if (j > r2) b2.y = -b2.y;
+          if (e & 1) { cfma(q1, b1, uj[e]); cfma(q2, b2, uj[e]); }
+          else { cfma(p1, b1, uj[e]); cfma(p2, b2, uj[e]); }
+        }
       }
-      cb += o + j + 1;
     }
-    p1 = cscale(p1, t);
-    p2 = cscale(p2, t);
+    p1 = rp.i1 >= 0 ? cscale(cadd(p1, q1), t) : z;
+    p2 = rp.i2 >= 0 ? cscale(cadd(p2, q2), t) : z;
     const float dp = wsum(x1.x * p1.x + x1.y * p1.y + x2.x * p2.x + x2.y * p2.y);
     const float K = 0.5f * t * dp;
     const float2 w1 = csub(p1, cscale(x1, K)), w2 = csub(p2, cscale(x2, K));
     if (rp.i1 >= 0) W->w[rp.i1] = w1;
     if (rp.i2 >= 0) W->w[rp.i2] = w2;
     __syncwarp();
-    // A22 -= u w^H + w u^H on the lower triangle of the lane's rows
+    // A22 -= u w^H + w u^H on the lower triangle of the lane's rows: element s of the lane is
+    // row i1 column s for s < n1, else row i2 column s - n1; every element has one owner lane,
+    // so the four loads of a group can all go out before its stores.
     const float2 nu1 = make_float2(-x1.x, -x1.y), nu2 = make_float2(-x2.x, -x2.y);
     const float2 nw1 = make_float2(-w1.x, -w1.y), nw2 = make_float2(-w2.x, -w2.y);
-    // one pass over both rows: the row switch happens once per lane, not as selects per element
-    float2 cu = nu1, cw = nw1;
-    int jo = 0, ib = rb1;
-    for (int s = 0; s < rp.tot; ++s) {
-      if (s == rp.n1) { cu = nu2; cw = nw2; jo = rp.n1; ib = rb2 - rp.n1; }
-      const int j = s - jo;
-      float2 a = A[ib + s];
-      cfma_cb(a, cu, W->w[j]);
-      cfma_cb(a, cw, W->u[j]);
-      A[ib + s] = a;
+    const int smax = max(rp.tot - 1, 0);
+    for (int s0 = 0; s0 <= L; s0 += 4) {
+      float2 a[4], wj[4], uj[4];
+      int id[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int sc = min(s0 + e, smax);
+        const bool f = sc < rp.n1;
+        const int j = f ? sc : sc - rp.n1;
+        id[e] = f ? rb1 + sc : rb2 + j;
+        a[e] = A[id[e]];
+        wj[e] = W->w[j];
+        uj[e] = W->u[j];
+      }
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const bool f = s0 + e < rp.n1;
+        float2 r = a[e];
+        cfma_cb(r, f ? nu1 : nu2, wj[e]);
+        cfma_cb(r, f ? nw1 : nw2, uj[e]);
+        if (s0 + e < rp.tot) A[id[e]] = r;
+      }
     }
     __syncwarp();
   }
@@ -310,20 +339,25 @@ __device__ bool warp_vectors(WarpEig<NPMAX>* W, int n, int ra, const TriInfo& ti
   }
   __syncwarp();
   if (lane < ra) {
-    float Lp[NPMAX], Um[NPMAX];
+    // Lp lives in the lane's own row of Y (overwritten in place by the vector), D+ / U- in the
+    // lane's row of um (the tridiagonalisation and Sturm scratch, dead by now).
+    float* y = W->Y + lane * NPMAX;
+    float* Um = W->um + lane * NPMAX;
     const float lam = W->lam[lane];
     float dp = W->d[0] - lam;
+#pragma unroll 4
     for (int i = 0; i + 1 < n; ++i) {
       if (fabsf(dp) < tiny) dp = copysignf(tiny, dp);
       Um[i] = dp;   // D+_i, replaced by U-_i on the way back
       const float l = W->ae[i] * __frcp_rn(dp);
-      Lp[i] = l;
+      y[i] = l;
       dp = W->d[i + 1] - lam - l * W->ae[i];
     }
     if (fabsf(dp) < tiny) dp = copysignf(tiny, dp);
     float dm = W->d[n - 1] - lam;
     float best = fabsf(dp);
     int r = n - 1;
+#pragma unroll 4
     for (int i = n - 2; i >= 0; --i) {
       if (fabsf(dm) < tiny) dm = copysignf(tiny, dm);
       const float um = W->ae[i] * __frcp_rn(dm);
@@ -333,10 +367,9 @@ __device__ bool warp_vectors(WarpEig<NPMAX>* W, int n, int ra, const TriInfo& ti
       const float gamma = dpi + dm - (W->d[i] - lam);
       if (fabsf(gamma) < best) { best = fabsf(gamma); r = i; }
     }
-    float* y = W->Y + lane * NPMAX;
     float zz = 1.f;
+    for (int i = r - 1; i >= 0; --i) { zz = -y[i] * zz; y[i] = zz; }
     y[r] = 1.f;
-    for (int i = r - 1; i >= 0; --i) { zz = -Lp[i] * zz; y[i] = zz; }
     zz = 1.f;
     for (int i = r; i + 1 < n; ++i) { zz = -Um[i] * zz; y[i + 1] = zz; }
     float mx = 0.f;
@@ -383,60 +416,57 @@ __device__ bool warp_vectors(WarpEig<NPMAX>* W, int n, int ra, const TriInfo& ti
   return !bad;
 }
 
-// V = Q D Y for all kept vectors at once (lane rows lane and lane + 32); written q-major to
-// fac[q * kFacCols + a].
+// V = Q D Y, Q = H_0 H_1 ... H_{n-3}: a group of Gv = 32 / R lanes per kept vector (R = ra
+// rounded up to a power of two), each lane holding the rows g, g + Gv, ... of its vector in
+// registers; per reflector a serial partial u^H v and log2(Gv) shuffle levels.  Written
+// q-major to fac[q * kFacCols + a].
 template <int NPMAX>
 __device__ void warp_backtransform(WarpEig<NPMAX>* W, int n, int ra, float2* fac) {
+  constexpr int kPer = NPMAX / 4;                 // rows per lane at Gv = 4 (ra > 4)
   const int lane = threadIdx.x & 31;
-  const int i0 = lane, i1 = lane + 32;
-  float2 v0[kFacCols], v1[kFacCols];
+  const int R = ra <= 1 ? 1 : (ra <= 2 ? 2 : (ra <= 4 ? 4 : 8));
+  const int Gv = 32 / R;
+  const int a = lane / Gv, g = lane - a * Gv;
+  const bool act = a < ra;
+  const int tmax = (n + Gv - 1) / Gv;             // warp-uniform
+  const float2 z = make_float2(0.f, 0.f);
+  float2 v[kPer];
 #pragma unroll
-  for (int a = 0; a < kFacCols; ++a) {
-    v0[a] = make_float2(0.f, 0.f);
-    v1[a] = make_float2(0.f, 0.f);
-    if (a < ra) {
-      if (i0 < n) v0[a] = cscale(W->delta[i0], W->Y[a * NPMAX + i0]);
-      if (i1 < n) v1[a] = cscale(W->delta[i1], W->Y[a * NPMAX + i1]);
-    }
+  for (int t = 0; t < kPer; ++t) {
+    const int i = g + Gv * t;
+    v[t] = (act && i < n) ? cscale(W->delta[i], W->Y[a * NPMAX + i]) : z;
   }
   for (int k = n - 3; k >= 0; --k) {
-    const float t = W->tau[k];
-    if (t == 0.f) continue;
-    const float2 u0 = (i0 > k && i0 < n) ? W->A[pk(i0, k)] : make_float2(0.f, 0.f);
-    const float2 u1 = (i1 > k && i1 < n) ? W->A[pk(i1, k)] : make_float2(0.f, 0.f);
-    float2 sv[kFacCols];
+    const float tk = W->tau[k];
+    if (tk == 0.f) continue;                      // warp-uniform
+    float2 s = z;
 #pragma unroll
-    for (int a = 0; a < kFacCols; ++a) sv[a] = cadd(cmulc(u0, v0[a]), cmulc(u1, v1[a]));
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-#pragma unroll
-      for (int a = 0; a < kFacCols; ++a) {
-        if (a < ra) {
-          sv[a].x += __shfl_xor_sync(0xffffffffu, sv[a].x, o);
-          sv[a].y += __shfl_xor_sync(0xffffffffu, sv[a].y, o);
-        }
-      }
+    for (int t = 0; t < kPer; ++t) {
+      if (t >= tmax) break;
+      const int i = g + Gv * t;
+      if (i > k && i < n) s = cadd(s, cmulc(W->A[pk(i, k)], v[t]));
     }
+    for (int o = Gv >> 1; o > 0; o >>= 1) {
+      s.x += __shfl_xor_sync(0xffffffffu, s.x, o);
+      s.y += __shfl_xor_sync(0xffffffffu, s.y, o);
+    }
+    s = cscale(s, tk);
 #pragma unroll
-    for (int a = 0; a < kFacCols; ++a) {
-      if (a < ra) {
-        const float2 s = cscale(sv[a], t);
-        v0[a] = csub(v0[a], cmul(u0, s));
-        v1[a] = csub(v1[a], cmul(u1, s));
-      }
+    for (int t = 0; t < kPer; ++t) {
+      if (t >= tmax) break;
+      const int i = g + Gv * t;
+      if (i > k && i < n) v[t] = csub(v[t], cmul(W->A[pk(i, k)], s));
     }
   }
 #pragma unroll
-  for (int a = 0; a < kFacCols; ++a) {
-    if (a < ra) {
-      if (i0 < n) fac[i0 * kFacCols + a] = v0[a];
-      if (i1 < n) fac[i1 * kFacCols + a] = v1[a];
-    }
+  for (int t = 0; t < kPer; ++t) {
+    const int i = g + Gv * t;
+    if (act && i < n) fac[i * kFacCols + a] = v[t];
   }
 }
 
 template <int NPMAX>
-__global__ void __launch_bounds__(32 * kEigWarps) llr_eig_warp_kernel(ProxOp op, long long nblocks) {
+__global__ void __launch_bounds__(32 * kEigWarps, 5) llr_eig_warp_kernel(ProxOp op, long long nblocks) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   WarpEig<NPMAX>* W = reinterpret_cast<WarpEig<NPMAX>*>(smem) + wib;
