@@ -27,16 +27,18 @@ constexpr int kKB = kKC / 4;               // 16-byte K groups per chunk
 constexpr int kOpBytes = 128 * kKC * 4;    // one operand plane (hi or lo) of one chunk
 constexpr unsigned long long kWaitLimit = 1ull << 22;   // bounded spin: ~seconds, never forever
 
-struct TcRowTab {
-  int off;
-  int cx;
-  int cyz;
-  int pad;
+// Row table of one block: planar offset of every row and either the row's phase (uniform
+// over the volumes) or its coordinates (per-volume phase).  The kernel keeps kRowBufs tables:
+// the one of the block being converted and those of the blocks whose chunks are prefetched.
+union TcRowAux {
+  float2 ph;
+  int2 c;              // x, y | z << 16
 };
 
 struct TcLayout {
-  size_t off_hdr, off_row, off_rowph, off_op, total;
+  size_t off_hdr, off_row, off_aux, off_op, total;
   int op_bytes;        // bytes of the operand / P-staging region
+  int nbuf;            // row tables: 2 (3 when a block is a single chunk)
 };
 
 struct TcHdr {
@@ -97,16 +99,16 @@ __device__ __forceinline__ uint32_t tf32_rna(float x) {
 __device__ __forceinline__ int op_offset(int mn, int kb) { return ((mn >> 3) * kKB + kb) * 128 + (mn & 7) * 16; }
 
 template <int NPMAX>
-__global__ void __launch_bounds__(kTcThreads, 2) llr_gram_tc_kernel(BlockSource src, ProxOp op, TcLayout L) {
+__global__ void __launch_bounds__(kTcThreads, 3) llr_gram_tc_kernel(BlockSource src, ProxOp op, TcLayout L) {
   extern __shared__ __align__(1024) unsigned char smem[];
   TcHdr* hdr = reinterpret_cast<TcHdr*>(smem + L.off_hdr);
-  TcRowTab* rows = reinterpret_cast<TcRowTab*>(smem + L.off_row);
-  float2* rowph = reinterpret_cast<float2*>(smem + L.off_rowph);
+  int* row_off = reinterpret_cast<int*>(smem + L.off_row);        // [nbuf][m]
+  TcRowAux* row_aux = reinterpret_cast<TcRowAux*>(smem + L.off_aux);   // [nbuf][m]
   unsigned char* ops = smem + L.off_op;   // [buf][hi, lo] planes; reused as P staging
   const int m = op.m, n = op.n, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const long long qstride = src.kind == 1 ? src.g.V : (long long)m;
-  const long long Pn = (long long)n * (n + 1) / 2;
   const int nchunks = (m + kKC - 1) / kKC;
+  const int nbuf = L.nbuf, la = nbuf - 1;   // row-table lookahead in blocks
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&hdr->tmem)),
@@ -131,34 +133,38 @@ __global__ void __launch_bounds__(kTcThreads, 2) llr_gram_tc_kernel(BlockSource 
   // Lane layout of the gather: 8 volumes x 4 consecutive rows per warp instruction, so one
   // request covers 8 short runs of the planar layout; warp w owns volume groups 2w and 2w+1.
   // In shared memory the same lanes write 32 consecutive words of one core-matrix row block.
+  // Chunks form one stream over the CTA's blocks; two register sets alternate, and after a
+  // set is converted it is refilled with the chunk two positions ahead, so two chunks of
+  // loads are in flight while the tensor core and the epilogue run.
   const int qsub = lane >> 2, usub = lane & 3;
-  float2 pre[2][kKB];
-  auto build_rows = [&](long long b) {
+  float2 preA[2][kKB], preB[2][kKB];
+  auto build_rows = [&](long long b, int buf) {
+    int* ro = row_off + (size_t)buf * m;
+    TcRowAux* ra = row_aux + (size_t)buf * m;
     for (int r = tid; r < m; r += kTcThreads) {
-      TcRowTab rt;
       if (src.kind == 1) {
         int ix, iy, iz;
         block_row_coord(src, b, sh, r, ix, iy, iz);
-        rt.off = (int)planar_index(src.g, ix, iy, iz, 0);
-        rt.cx = ix;
-        rt.cyz = iy | (iz << 16);
-        if (src.ph_uniform) rowph[r] = phase_at(src.ph, src.g, 0, ix, iy, iz);
+        ro[r] = (int)planar_index(src.g, ix, iy, iz, 0);
+        TcRowAux a;
+        if (src.ph_uniform) a.ph = phase_at(src.ph, src.g, 0, ix, iy, iz);
+        else a.c = make_int2(ix, iy | (iz << 16));
+        ra[r] = a;
       } else {
-        rt.off = r;
-        rt.cx = 0;
-        rt.cyz = 0;
+        ro[r] = r;
       }
-      rt.pad = 0;
-      rows[r] = rt;
     }
   };
-  auto load_chunk = [&](int c, long long base) {
+  auto block_base = [&](long long b) { return src.kind == 1 ? 0ll : b * (long long)m * n; };
+  auto load_chunk = [&](float2 (&pre)[2][kKB], int c, long long b, int buf) {
     const int c0 = c * kKC;
+    const int* ro = row_off + (size_t)buf * m;
+    const long long base = block_base(b);
     int roff[kKB];
 #pragma unroll
     for (int kb = 0; kb < kKB; ++kb) {
       const int r = c0 + 4 * kb + usub;
-      roff[kb] = r < m ? rows[r].off : -1;
+      roff[kb] = r < m ? ro[r] : -1;
     }
 #pragma unroll
     for (int t = 0; t < 2; ++t) {
@@ -169,82 +175,104 @@ __global__ void __launch_bounds__(kTcThreads, 2) llr_gram_tc_kernel(BlockSource 
         pre[t][kb] = (q < n && roff[kb] >= 0) ? col[roff[kb]] : make_float2(0.f, 0.f);
     }
   };
-  auto block_base = [&](long long b) { return src.kind == 1 ? 0ll : b * (long long)m * n; };
+  // the chunk `ahead` positions after (block iteration j, chunk c); false past the CTA's blocks
+  auto locate = [&](long long blk, int j, int c, int ahead, long long& b2, int& j2, int& c2) {
+    c2 = c + ahead;
+    j2 = j;
+    b2 = blk;
+    while (c2 >= nchunks) { c2 -= nchunks; ++j2; b2 += gridDim.x; }
+    return b2 < src.nblocks;
+  };
+  // one chunk: wait for its operand buffer, convert `pre` into it, refill `pre` two chunks
+  // ahead, hand the buffer to the tensor core
+  int gpar = 0;
+  auto step = [&](float2 (&pre)[2][kKB], long long blk, int j, int c) -> bool {
+    const int b = gpar;
+    if (used[b]) {  // the MMAs that read this buffer two chunks ago must be done
+      const bool ok = mbar_wait(smem_u32(&hdr->mbar[b]), phase[b]);
+      phase[b] ^= 1u;
+      if (__syncthreads_or(!ok)) return false;
+    }
+    unsigned char* hi = ops + (size_t)b * 2 * kOpBytes;
+    unsigned char* lo = hi + kOpBytes;
+    const int c0 = c * kKC;
+    const TcRowAux* ra = row_aux + (size_t)(j % nbuf) * m;
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      const int q = 8 * (2 * warp + t) + qsub;
+      if (q >= n) continue;
+#pragma unroll
+      for (int kb = 0; kb < kKB; ++kb) {
+        const int r = c0 + 4 * kb + usub;
+        float2 x = pre[t][kb];
+        if (src.kind == 1 && r < m) {
+          float2 p;
+          if (src.ph_uniform) p = ra[r].ph;
+          else {
+            const int2 cc = ra[r].c;
+            p = phase_at(src.ph, src.g, q, cc.x, cc.y & 0xffff, cc.y >> 16);
+          }
+          x = cscale(cmul_bc(x, p), src.load_scale);
+        }
+        const uint32_t a = tf32_rna(x.x), bb = tf32_rna(x.y);
+        const int oq = op_offset(q, kb) + 4 * usub, oi = op_offset(n + q, kb) + 4 * usub;
+        *reinterpret_cast<uint32_t*>(hi + oq) = a;
+        *reinterpret_cast<uint32_t*>(hi + oi) = bb;
+        *reinterpret_cast<uint32_t*>(lo + oq) = __float_as_uint(x.x - __uint_as_float(a));
+        *reinterpret_cast<uint32_t*>(lo + oi) = __float_as_uint(x.y - __uint_as_float(bb));
+      }
+    }
+    {
+      long long b2;
+      int j2, c2;
+      if (locate(blk, j, c, 2, b2, j2, c2)) load_chunk(pre, c2, b2, j2 % nbuf);
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      const uint32_t ah = smem_u32(hi), al = smem_u32(lo);
+#pragma unroll
+      for (int s = 0; s < kKC / 8; ++s) {
+        const uint64_t dh = umma_desc(ah + s * 256, 128, kKB * 128);
+        const uint64_t dl = umma_desc(al + s * 256, 128, kKB * 128);
+        umma_tf32(tmem, dh, dh, (c > 0 || s > 0) ? 1u : 0u);
+        umma_tf32(tmem, dh, dl, 1u);
+        umma_tf32(tmem, dl, dh, 1u);
+      }
+      umma_commit(smem_u32(&hdr->mbar[b]));
+      if (c == nchunks - 1) umma_commit(smem_u32(&hdr->mbar[2]));
+    }
+    used[b] = true;
+    gpar ^= 1;
+    return true;
+  };
 
   // operand planes start zeroed: rows 2n..127 (M padding) are never written by the gather
   for (int i = tid; i < 4 * kOpBytes / 16; i += kTcThreads)
     reinterpret_cast<float4*>(ops)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
   long long blk = blockIdx.x;
   if (blk < src.nblocks) {
-    build_rows(blk);
+    for (int jj = 0; jj <= la; ++jj)
+      if (blk + (long long)jj * gridDim.x < src.nblocks) build_rows(blk + (long long)jj * gridDim.x, jj % nbuf);
     __syncthreads();
-    load_chunk(0, block_base(blk));
+    long long b2;
+    int j2, c2;
+    if (locate(blk, 0, 0, 0, b2, j2, c2)) load_chunk(preA, c2, b2, j2 % nbuf);
+    if (locate(blk, 0, 0, 1, b2, j2, c2)) load_chunk(preB, c2, b2, j2 % nbuf);
   }
 
-  for (; blk < src.nblocks && !failed; blk += gridDim.x) {
-    const long long nxt = blk + gridDim.x;
-    for (int c = 0; c < nchunks; ++c) {
-      const int b = c & 1;
-      if (used[b]) {  // the MMAs that read this buffer two chunks ago must be done
-        const bool ok = mbar_wait(smem_u32(&hdr->mbar[b]), phase[b]);
-        phase[b] ^= 1u;
-        if (__syncthreads_or(!ok)) { failed = true; break; }
-      }
-      unsigned char* hi = ops + (size_t)b * 2 * kOpBytes;
-      unsigned char* lo = hi + kOpBytes;
-      const int c0 = c * kKC;
-#pragma unroll
-      for (int t = 0; t < 2; ++t) {
-        const int q = 8 * (2 * warp + t) + qsub;
-        if (q >= n) continue;
-#pragma unroll
-        for (int kb = 0; kb < kKB; ++kb) {
-          const int r = c0 + 4 * kb + usub;
-          float2 x = pre[t][kb];
-          if (src.kind == 1 && r < m) {
-            float2 p;
-            if (src.ph_uniform) p = rowph[r];
-            else {
-              const TcRowTab rt = rows[r];
-              p = phase_at(src.ph, src.g, q, rt.cx, rt.cyz & 0xffff, rt.cyz >> 16);
-            }
-            x = cscale(cmul_bc(x, p), src.load_scale);
-          }
-          const uint32_t a = tf32_rna(x.x), bb = tf32_rna(x.y);
-          const int oq = op_offset(q, kb) + 4 * usub, oi = op_offset(n + q, kb) + 4 * usub;
-          *reinterpret_cast<uint32_t*>(hi + oq) = a;
-          *reinterpret_cast<uint32_t*>(hi + oi) = bb;
-          *reinterpret_cast<uint32_t*>(lo + oq) = __float_as_uint(x.x - __uint_as_float(a));
-          *reinterpret_cast<uint32_t*>(lo + oi) = __float_as_uint(x.y - __uint_as_float(bb));
-        }
-      }
-      if (c + 1 < nchunks) load_chunk(c + 1, block_base(blk));   // in flight while the tensor core works
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  for (int j = 0; blk < src.nblocks && !failed; blk += gridDim.x, ++j) {
+    if (j > 0) {   // the table of the block `la` ahead goes into the buffer the previous block freed
+      const long long bl = blk + (long long)la * gridDim.x;
+      if (bl < src.nblocks) build_rows(bl, (j + la) % nbuf);
       __syncthreads();
-      if (tid == 0) {
-        asm volatile("tcgen05.fence::after_thread_sync;");
-        const uint32_t ah = smem_u32(hi), al = smem_u32(lo);
-#pragma unroll
-        for (int s = 0; s < kKC / 8; ++s) {
-          const uint64_t dh = umma_desc(ah + s * 256, 128, kKB * 128);
-          const uint64_t dl = umma_desc(al + s * 256, 128, kKB * 128);
-          umma_tf32(tmem, dh, dh, (c > 0 || s > 0) ? 1u : 0u);
-          umma_tf32(tmem, dh, dl, 1u);
-          umma_tf32(tmem, dl, dh, 1u);
-        }
-        umma_commit(smem_u32(&hdr->mbar[b]));
-        if (c == nchunks - 1) umma_commit(smem_u32(&hdr->mbar[2]));
-      }
-      used[b] = true;
+    }
+    for (int c = 0; c < nchunks; ++c) {
+      const bool ok = gpar == 0 ? step(preA, blk, j, c) : step(preB, blk, j, c);
+      if (!ok) { failed = true; break; }
     }
     if (failed) break;
-    // the row table is free once the last chunk is converted: the next block's table and its
-    // first chunk's loads go out now and overlap the MMAs' tail and this block's epilogue
-    if (nxt < src.nblocks) {
-      build_rows(nxt);
-      __syncthreads();
-      load_chunk(0, block_base(nxt));
-    }
     // all MMAs of this block complete -> read P and stage it in the (now idle) operand area
     {
       const bool ok = mbar_wait(smem_u32(&hdr->mbar[2]), phase[2]);
@@ -275,20 +303,21 @@ __global__ void __launch_bounds__(kTcThreads, 2) llr_gram_tc_kernel(BlockSource 
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
       if (a < 2 * n) {
 #pragma unroll
-        for (int j = 0; j < 32; ++j)
-          if (cc + j < 2 * n) Ps[a * ldp + cc + j] = __uint_as_float(r[j]);
+        for (int jj = 0; jj < 32; ++jj)
+          if (cc + jj < 2 * n) Ps[a * ldp + cc + jj] = __uint_as_float(r[jj]);
       }
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
+    // packed lower triangle, row i of G by one warp (rows round-robin over the warps)
     float2* G = op.gram + blk * op.gram_stride;
-    for (long long idx = tid; idx < Pn; idx += kTcThreads) {
-      const int i = (int)((sqrtf(8.f * (float)idx + 1.f) - 1.f) * 0.5f);
-      const int ii = ((long long)i * (i + 1) / 2 > idx) ? i - 1 : (((long long)(i + 1) * (i + 2) / 2 <= idx) ? i + 1 : i);
-      const int j = (int)(idx - (long long)ii * (ii + 1) / 2);
-      const float re = Ps[ii * ldp + j] + Ps[(n + ii) * ldp + n + j];
-      const float im = Ps[ii * ldp + n + j] - Ps[(n + ii) * ldp + j];
-      G[idx] = make_float2(re, im);
+    for (int i = warp; i < n; i += kTcThreads / 32) {
+      float2* Gi = G + (long long)i * (i + 1) / 2;
+      for (int jj = lane; jj <= i; jj += 32) {
+        const float re = Ps[i * ldp + jj] + Ps[(n + i) * ldp + n + jj];
+        const float im = Ps[i * ldp + n + jj] - Ps[(n + i) * ldp + jj];
+        Gi[jj] = make_float2(re, im);
+      }
     }
     __syncthreads();
     // the staging overwrote the padding rows 2n..127 of the operand planes: zero them again
@@ -316,8 +345,9 @@ TcLayout make_tc_layout(int m, int n) {
   TcLayout L;
   size_t off = 0;
   L.off_hdr = off; off = align16(off + sizeof(TcHdr));
-  L.off_row = off; off = align16(off + sizeof(TcRowTab) * (size_t)m);
-  L.off_rowph = off; off = align16(off + sizeof(float2) * (size_t)m);
+  L.nbuf = m <= kKC ? 3 : 2;
+  L.off_row = off; off = align16(off + sizeof(int) * (size_t)m * L.nbuf);
+  L.off_aux = off; off = align16(off + sizeof(TcRowAux) * (size_t)m * L.nbuf);
   off = (off + 1023) & ~size_t(1023);
   L.off_op = off;
   const size_t opb = std::max<size_t>(4 * (size_t)kOpBytes, sizeof(float) * (size_t)(2 * n) * (2 * n + 1));
