@@ -23,7 +23,7 @@ namespace {
 
 constexpr int kTcThreads = 128;
 constexpr int kKC = 32;                    // rows (K) per staged chunk
-constexpr int kKB = kKC / 4;               // 16-byte K groups per chunk
+constexpr int kQT = 16;                    // volumes per warp per chunk (4 warps x 16 >= n)
 constexpr int kOpBytes = 128 * kKC * 4;    // one operand plane (hi or lo) of one chunk
 constexpr unsigned long long kWaitLimit = 1ull << 22;   // bounded spin: ~seconds, never forever
 
@@ -51,12 +51,15 @@ struct TcHdr {
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-// K-major, no-swizzle UMMA shared-memory descriptor (sm_100 version 1).
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+// K-major UMMA shared-memory descriptor (sm_100 version 1) with the 128-byte swizzle: rows of
+// 128 B (32 TF32 along K), 8-row atoms of 1 KB (SBO = 1 KB), the 16-byte chunk index XORed with
+// the row index inside the atom.  Stepping K by 8 TF32 moves the start address by 32 B.
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
   uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
-  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
-  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 16;                          // LBO: unused for swizzled K-major
+  d |= (uint64_t)(1024u >> 4) << 32;               // SBO: next 8-row atom
   d |= (uint64_t)1 << 46;
+  d |= (uint64_t)2 << 61;                          // SWIZZLE_128B
   return d;
 }
 
@@ -95,8 +98,10 @@ __device__ __forceinline__ uint32_t tf32_rna(float x) {
   return r;
 }
 
-// Element (mn, k) of one operand plane: core matrix (mn/8, k/4) of 8 rows x 16 bytes.
-__device__ __forceinline__ int op_offset(int mn, int kb) { return ((mn >> 3) * kKB + kb) * 128 + (mn & 7) * 16; }
+// Byte offset of element (mn, k) of one operand plane (k < 32) in the 128-byte swizzled layout.
+__device__ __forceinline__ int op_offset(int mn, int k) {
+  return (mn >> 3) * 1024 + (mn & 7) * 128 + ((((k >> 2) ^ mn) & 7) << 4) + ((k & 3) << 2);
+}
 
 template <int NPMAX>
 __global__ void __launch_bounds__(kTcThreads, 3) llr_gram_tc_kernel(BlockSource src, ProxOp op, TcLayout L) {
@@ -130,14 +135,14 @@ __global__ void __launch_bounds__(kTcThreads, 3) llr_gram_tc_kernel(BlockSource 
   bool used[2] = {false, false};
   bool failed = false;
 
-  // Lane layout of the gather: 8 volumes x 4 consecutive rows per warp instruction, so one
-  // request covers 8 short runs of the planar layout; warp w owns volume groups 2w and 2w+1.
-  // In shared memory the same lanes write 32 consecutive words of one core-matrix row block.
+  // Lane layout of the gather: lane = row of the chunk, warp w = volumes w, w + 4, ...: every
+  // request reads 32 consecutive rows of one volume (the block's runs along y of one DRAM
+  // page); requests that mix volumes, one short run each, reach a fraction of the HBM rate.
+  // In shared memory the 32 lanes write one 128-byte swizzled row (all banks).
   // Chunks form one stream over the CTA's blocks; two register sets alternate, and after a
   // set is converted it is refilled with the chunk two positions ahead, so two chunks of
   // loads are in flight while the tensor core and the epilogue run.
-  const int qsub = lane >> 2, usub = lane & 3;
-  float2 preA[2][kKB], preB[2][kKB];
+  float2 preA[kQT], preB[kQT];
   auto build_rows = [&](long long b, int buf) {
     int* ro = row_off + (size_t)buf * m;
     TcRowAux* ra = row_aux + (size_t)buf * m;
@@ -156,23 +161,14 @@ __global__ void __launch_bounds__(kTcThreads, 3) llr_gram_tc_kernel(BlockSource 
     }
   };
   auto block_base = [&](long long b) { return src.kind == 1 ? 0ll : b * (long long)m * n; };
-  auto load_chunk = [&](float2 (&pre)[2][kKB], int c, long long b, int buf) {
-    const int c0 = c * kKC;
-    const int* ro = row_off + (size_t)buf * m;
-    const long long base = block_base(b);
-    int roff[kKB];
+  auto load_chunk = [&](float2 (&pre)[kQT], int c, long long b, int buf) {
+    const int r = c * kKC + lane;
+    const int ro = r < m ? row_off[(size_t)buf * m + r] : -1;
+    const float2* rowp = src.data + block_base(b) + (ro >= 0 ? ro : 0);
 #pragma unroll
-    for (int kb = 0; kb < kKB; ++kb) {
-      const int r = c0 + 4 * kb + usub;
-      roff[kb] = r < m ? ro[r] : -1;
-    }
-#pragma unroll
-    for (int t = 0; t < 2; ++t) {
-      const int q = 8 * (2 * warp + t) + qsub;
-      const float2* col = src.data + base + (long long)q * qstride;
-#pragma unroll
-      for (int kb = 0; kb < kKB; ++kb)
-        pre[t][kb] = (q < n && roff[kb] >= 0) ? col[roff[kb]] : make_float2(0.f, 0.f);
+    for (int t = 0; t < kQT; ++t) {
+      const int q = warp + 4 * t;
+      pre[t] = (q < n && ro >= 0) ? rowp[(long long)q * qstride] : make_float2(0.f, 0.f);
     }
   };
   // the chunk `ahead` positions after (block iteration j, chunk c); false past the CTA's blocks
@@ -186,7 +182,7 @@ __global__ void __launch_bounds__(kTcThreads, 3) llr_gram_tc_kernel(BlockSource 
   // one chunk: wait for its operand buffer, convert `pre` into it, refill `pre` two chunks
   // ahead, hand the buffer to the tensor core
   int gpar = 0;
-  auto step = [&](float2 (&pre)[2][kKB], long long blk, int j, int c) -> bool {
+  auto step = [&](float2 (&pre)[kQT], long long blk, int j, int c) -> bool {
     const int b = gpar;
     if (used[b]) {  // the MMAs that read this buffer two chunks ago must be done
       const bool ok = mbar_wait(smem_u32(&hdr->mbar[b]), phase[b]);
@@ -195,32 +191,29 @@ __global__ void __launch_bounds__(kTcThreads, 3) llr_gram_tc_kernel(BlockSource 
     }
     unsigned char* hi = ops + (size_t)b * 2 * kOpBytes;
     unsigned char* lo = hi + kOpBytes;
-    const int c0 = c * kKC;
+    const int r = c * kKC + lane;
     const TcRowAux* ra = row_aux + (size_t)(j % nbuf) * m;
+    const bool ph_row = src.kind == 1 && r < m;
+    float2 p = make_float2(1.f, 0.f);
+    if (ph_row && src.ph_uniform) p = ra[r].ph;
 #pragma unroll
-    for (int t = 0; t < 2; ++t) {
-      const int q = 8 * (2 * warp + t) + qsub;
-      if (q >= n) continue;
-#pragma unroll
-      for (int kb = 0; kb < kKB; ++kb) {
-        const int r = c0 + 4 * kb + usub;
-        float2 x = pre[t][kb];
-        if (src.kind == 1 && r < m) {
-          float2 p;
-          if (src.ph_uniform) p = ra[r].ph;
-          else {
-            const int2 cc = ra[r].c;
-            p = phase_at(src.ph, src.g, q, cc.x, cc.y & 0xffff, cc.y >> 16);
-          }
-          x = cscale(cmul_bc(x, p), src.load_scale);
+    for (int t = 0; t < kQT; ++t) {
+      const int q = warp + 4 * t;
+      if (q >= n) break;                              // warp-uniform
+      float2 x = pre[t];
+      if (ph_row) {
+        if (!src.ph_uniform) {
+          const int2 cc = ra[r].c;
+          p = phase_at(src.ph, src.g, q, cc.x, cc.y & 0xffff, cc.y >> 16);
         }
-        const uint32_t a = tf32_rna(x.x), bb = tf32_rna(x.y);
-        const int oq = op_offset(q, kb) + 4 * usub, oi = op_offset(n + q, kb) + 4 * usub;
-        *reinterpret_cast<uint32_t*>(hi + oq) = a;
-        *reinterpret_cast<uint32_t*>(hi + oi) = bb;
-        *reinterpret_cast<uint32_t*>(lo + oq) = __float_as_uint(x.x - __uint_as_float(a));
-        *reinterpret_cast<uint32_t*>(lo + oi) = __float_as_uint(x.y - __uint_as_float(bb));
+        x = cscale(cmul_bc(x, p), src.load_scale);
       }
+      const uint32_t a = tf32_rna(x.x), bb = tf32_rna(x.y);
+      const int oq = op_offset(q, lane), oi = op_offset(n + q, lane);
+      *reinterpret_cast<uint32_t*>(hi + oq) = a;
+      *reinterpret_cast<uint32_t*>(hi + oi) = bb;
+      *reinterpret_cast<uint32_t*>(lo + oq) = __float_as_uint(x.x - __uint_as_float(a));
+      *reinterpret_cast<uint32_t*>(lo + oi) = __float_as_uint(x.y - __uint_as_float(bb));
     }
     {
       long long b2;
@@ -234,8 +227,8 @@ __global__ void __launch_bounds__(kTcThreads, 3) llr_gram_tc_kernel(BlockSource 
       const uint32_t ah = smem_u32(hi), al = smem_u32(lo);
 #pragma unroll
       for (int s = 0; s < kKC / 8; ++s) {
-        const uint64_t dh = umma_desc(ah + s * 256, 128, kKB * 128);
-        const uint64_t dl = umma_desc(al + s * 256, 128, kKB * 128);
+        const uint64_t dh = umma_desc_sw128(ah + s * 32);
+        const uint64_t dl = umma_desc_sw128(al + s * 32);
         umma_tf32(tmem, dh, dh, (c > 0 || s > 0) ? 1u : 0u);
         umma_tf32(tmem, dh, dl, 1u);
         umma_tf32(tmem, dl, dh, 1u);
@@ -321,10 +314,11 @@ __global__ void __launch_bounds__(kTcThreads, 3) llr_gram_tc_kernel(BlockSource 
     }
     __syncthreads();
     // the staging overwrote the padding rows 2n..127 of the operand planes: zero them again
-    for (int i = tid; i < 4 * (128 - 2 * n) * kKB; i += kTcThreads) {
-      const int plane = i / ((128 - 2 * n) * kKB), rem = i - plane * ((128 - 2 * n) * kKB);
-      const int mn = 2 * n + rem / kKB, kb = rem - (rem / kKB) * kKB;
-      *reinterpret_cast<float4*>(ops + (size_t)plane * kOpBytes + op_offset(mn, kb)) = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int i = tid; i < 4 * (128 - 2 * n) * 8; i += kTcThreads) {   // 8 x 16 B per 128-B row
+      const int plane = i / ((128 - 2 * n) * 8), rem = i - plane * ((128 - 2 * n) * 8);
+      const int mn = 2 * n + (rem >> 3), c16 = rem & 7;
+      *reinterpret_cast<float4*>(ops + (size_t)plane * kOpBytes + (mn >> 3) * 1024 + (mn & 7) * 128 + c16 * 16) =
+          make_float4(0.f, 0.f, 0.f, 0.f);
     }
     __syncthreads();
   }
