@@ -92,10 +92,10 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
   return false;
 }
 
+// TF32 part of x rounded to nearest (ties away from zero) on the 10-bit mantissa: add half a
+// TF32 unit to the magnitude bits and clear the 13 low bits.  Finite inputs only (the iterate).
 __device__ __forceinline__ uint32_t tf32_rna(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return r;
+  return (__float_as_uint(x) + 0x1000u) & 0xFFFFE000u;
 }
 
 // Byte offset of element (mn, k) of one operand plane (k < 32) in the 128-byte swizzled layout.
@@ -302,14 +302,25 @@ __global__ void __launch_bounds__(kTcThreads, 3) llr_gram_tc_kernel(BlockSource 
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
-    // packed lower triangle, row i of G by one warp (rows round-robin over the warps)
+    // packed lower triangle by row pairs (i, n - 1 - i): n + 1 elements per pair, so a warp's
+    // lanes stay busy; two elements per lane in flight
     float2* G = op.gram + blk * op.gram_stride;
-    for (int i = warp; i < n; i += kTcThreads / 32) {
-      float2* Gi = G + (long long)i * (i + 1) / 2;
-      for (int jj = lane; jj <= i; jj += 32) {
-        const float re = Ps[i * ldp + jj] + Ps[(n + i) * ldp + n + jj];
-        const float im = Ps[i * ldp + n + jj] - Ps[(n + i) * ldp + jj];
-        Gi[jj] = make_float2(re, im);
+    for (int i = warp; i < (n + 1) / 2; i += kTcThreads / 32) {
+      const int i2 = n - 1 - i, len = i2 == i ? i + 1 : n + 1;
+      for (int s0 = lane; s0 < len; s0 += 64) {
+        float re[2], im[2];
+        int row[2], col[2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int s = min(s0 + 32 * u, len - 1);
+          row[u] = s <= i ? i : i2;
+          col[u] = s <= i ? s : s - i - 1;
+          re[u] = Ps[row[u] * ldp + col[u]] + Ps[(n + row[u]) * ldp + n + col[u]];
+          im[u] = Ps[row[u] * ldp + n + col[u]] - Ps[(n + row[u]) * ldp + col[u]];
+        }
+#pragma unroll
+        for (int u = 0; u < 2; ++u)
+          if (s0 + 32 * u < len) G[(long long)row[u] * (row[u] + 1) / 2 + col[u]] = make_float2(re[u], im[u]);
       }
     }
     __syncthreads();

@@ -427,16 +427,30 @@ struct RowTab {
   int pad;
 };
 
-__device__ __forceinline__ float2 load_elem(const BlockSource& s, long long base, const RowTab& rt, const float2* rowph,
-                                            int r, int q, long long qstride) {
-  float2 v = s.data[base + (long long)rt.off + (long long)q * qstride];
+// KB raw loads of row r (volumes k0 .. k0 + KB - 1) with nothing between them, then the phase
+// correction: the loads are all in flight before the first use (a per-element branch between
+// them would serialise the round trips).
+template <int KB>
+__device__ __forceinline__ void load_row_batch(const BlockSource& s, long long base, const RowTab& rt,
+                                               const float2* rowph, int r, int k0, int n, long long qstride,
+                                               float2 (&c)[KB]) {
+  const float2* rowp = s.data + base + (long long)rt.off;
+#pragma unroll
+  for (int u = 0; u < KB; ++u)
+    c[u] = (k0 + u < n) ? rowp[(long long)(k0 + u) * qstride] : make_float2(0.f, 0.f);
   if (s.kind == 1) {
-    float2 p;
-    if (s.ph_uniform) p = rowph[r];
-    else p = phase_at(s.ph, s.g, q, rt.cx, rt.cyz & 0xffff, rt.cyz >> 16);
-    v = cscale(cmul_bc(v, p), s.load_scale);
+    if (s.ph_uniform) {
+      const float2 p = rowph[r];
+#pragma unroll
+      for (int u = 0; u < KB; ++u) c[u] = cscale(cmul_bc(c[u], p), s.load_scale);
+    } else {
+#pragma unroll
+      for (int u = 0; u < KB; ++u)
+        if (k0 + u < n)
+          c[u] = cscale(cmul_bc(c[u], phase_at(s.ph, s.g, k0 + u, rt.cx, rt.cyz & 0xffff, rt.cyz >> 16)),
+                        s.load_scale);
+    }
   }
-  return v;
 }
 
 __device__ __forceinline__ void store_elem(const BlockSource& s, long long base, const RowTab& rt, const float2* rowph,
@@ -497,9 +511,7 @@ __device__ void apply_rows(const BlockSource& s, long long base, const RowTab* r
     for (int a = 0; a < RM; ++a) t[a] = make_float2(0.f, 0.f);
     for (int k0 = 0; k0 < n; k0 += KB) {
       float2 c[KB];
-#pragma unroll
-      for (int u = 0; u < KB; ++u)
-        c[u] = (k0 + u < n) ? load_elem(s, base, rt, rowph, r, k0 + u, qstride) : make_float2(0.f, 0.f);
+      load_row_batch<KB>(s, base, rt, rowph, r, k0, n, qstride, c);
 #pragma unroll
       for (int u = 0; u < KB; ++u) {
         if (k0 + u < n) {
@@ -926,9 +938,7 @@ __device__ void apply_rows_refined(const BlockSource& s, long long base, const R
       const RowTab rt = rows[r];
       for (int k0 = 0; k0 < n; k0 += KB) {
         float2 c[KB];
-#pragma unroll
-        for (int u = 0; u < KB; ++u)
-          c[u] = (k0 + u < n) ? load_elem(s, base, rt, rowph, r, k0 + u, qstride) : make_float2(0.f, 0.f);
+        load_row_batch<KB>(s, base, rt, rowph, r, k0, n, qstride, c);
 #pragma unroll
         for (int u = 0; u < KB; ++u) {
           if (k0 + u < n) {
@@ -997,7 +1007,7 @@ inline ApplyLayout make_apply_layout(int m, int n) {
   return L;
 }
 
-__global__ void __launch_bounds__(kApplyThreads, 4) llr_apply_kernel(BlockSource src, ProxOp op, ApplyLayout L) {
+__global__ void __launch_bounds__(kApplyThreads, 3) llr_apply_kernel(BlockSource src, ProxOp op, ApplyLayout L) {
   extern __shared__ __align__(16) unsigned char smem[];
   int* sh_s = reinterpret_cast<int*>(smem);
   RowTab* rows = reinterpret_cast<RowTab*>(smem + L.off_row);
@@ -1039,10 +1049,10 @@ __global__ void __launch_bounds__(kApplyThreads, 4) llr_apply_kernel(BlockSource
       if (tid < kFacCols) g[tid] = F[n * kFacCols + tid].x;
     }
     __syncthreads();
-    if (ra == 0) {
-      for (int idx = tid; idx < m * n; idx += blockDim.x) {
-        const int q = idx / m, r = idx - q * m;
-        store_elem(src, base, rows[r], rowph, r, q, qstride, make_float2(0.f, 0.f));
+    if (ra == 0) {   // every singular value below the threshold: the block becomes zero
+      for (int r = tid; r < m; r += blockDim.x) {
+        float2* rowp = src.data + base + (long long)rows[r].off;
+        for (int q = 0; q < n; ++q) rowp[(long long)q * qstride] = make_float2(0.f, 0.f);
       }
     } else if (refine) {
       if (ra <= 2) apply_rows_refined<2>(src, base, rows, rowph, m, n, qstride, Va, g, ra, op.lambda, red);
@@ -1063,7 +1073,8 @@ int launch_apply(const BlockSource& src, const ProxOp& op, cudaStream_t stream) 
   const ApplyLayout L = make_apply_layout(op.m, op.n);
   if (L.total > 227 * 1024) return set_error(LLR_ERR_UNSUPPORTED, "apply kernel needs %zu B smem", L.total);
   LLR_CUDA_TRY(cudaFuncSetAttribute(llr_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total));
-  // room for eight resident CTAs (the thread limit); the rest of the SM's memory stays L1
+  // shared memory for up to eight resident CTAs (the thread limit; registers allow three); the
+  // rest of the SM's memory stays L1
   const int carve = (int)std::min<size_t>(100, (8 * (L.total + 1024) * 100) / (228 * 1024) + 1);
   LLR_CUDA_TRY(cudaFuncSetAttribute(llr_apply_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
   const long long grid = std::min<long long>(src.nblocks, 1ll << 30);
