@@ -21,9 +21,10 @@ namespace llr {
 
 namespace {
 
-constexpr int kTcThreads = 128;
+constexpr int kTcWarps = 8;
+constexpr int kTcThreads = 32 * kTcWarps;
 constexpr int kKC = 32;                    // rows (K) per staged chunk
-constexpr int kQT = 16;                    // volumes per warp per chunk (4 warps x 16 >= n)
+constexpr int kQT = (64 + kTcWarps - 1) / kTcWarps;   // volumes per warp per chunk (kTcWarps x kQT >= n)
 constexpr int kOpBytes = 128 * kKC * 4;    // one operand plane (hi or lo) of one chunk
 constexpr unsigned long long kWaitLimit = 1ull << 22;   // bounded spin: ~seconds, never forever
 
@@ -135,7 +136,7 @@ __global__ void __launch_bounds__(kTcThreads, 3) llr_gram_tc_kernel(BlockSource 
   bool used[2] = {false, false};
   bool failed = false;
 
-  // Lane layout of the gather: lane = row of the chunk, warp w = volumes w, w + 4, ...: every
+  // Lane layout of the gather: lane = row of the chunk, warp w = volumes w, w + kTcWarps, ...: every
   // request reads 32 consecutive rows of one volume (the block's runs along y of one DRAM
   // page); requests that mix volumes, one short run each, reach a fraction of the HBM rate.
   // In shared memory the 32 lanes write one 128-byte swizzled row (all banks).
@@ -167,7 +168,7 @@ __global__ void __launch_bounds__(kTcThreads, 3) llr_gram_tc_kernel(BlockSource 
     const float2* rowp = src.data + block_base(b) + (ro >= 0 ? ro : 0);
 #pragma unroll
     for (int t = 0; t < kQT; ++t) {
-      const int q = warp + 4 * t;
+      const int q = warp + kTcWarps * t;
       pre[t] = (q < n && ro >= 0) ? rowp[(long long)q * qstride] : make_float2(0.f, 0.f);
     }
   };
@@ -198,7 +199,7 @@ __global__ void __launch_bounds__(kTcThreads, 3) llr_gram_tc_kernel(BlockSource 
     if (ph_row && src.ph_uniform) p = ra[r].ph;
 #pragma unroll
     for (int t = 0; t < kQT; ++t) {
-      const int q = warp + 4 * t;
+      const int q = warp + kTcWarps * t;
       if (q >= n) break;                              // warp-uniform
       float2 x = pre[t];
       if (ph_row) {
@@ -282,8 +283,11 @@ __global__ void __launch_bounds__(kTcThreads, 3) llr_gram_tc_kernel(BlockSource 
     asm volatile("tcgen05.fence::after_thread_sync;");
     float* Ps = reinterpret_cast<float*>(ops);
     const int ldp = 2 * n + 1;
-    const int a = 32 * warp + lane;          // accumulator row held by this thread
-    for (int cc = 0; cc < 2 * n; cc += 32) {
+    // warp w reads TMEM lanes 32 (w mod 4) .. + 31 (its quadrant); the warps sharing a quadrant
+    // split the 32-column chunks
+    const int quad = warp & 3;
+    const int a = 32 * quad + lane;          // accumulator row held by this thread
+    for (int cc = 32 * (warp >> 2); cc < 2 * n; cc += 32 * (kTcWarps / 4)) {
       uint32_t r[32];
       asm volatile(
           "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
@@ -292,7 +296,7 @@ __global__ void __launch_bounds__(kTcThreads, 3) llr_gram_tc_kernel(BlockSource 
             "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
             "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
             "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-          : "r"(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)cc));
+          : "r"(tmem + ((uint32_t)(32 * quad) << 16) + (uint32_t)cc));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
       if (a < 2 * n) {
 #pragma unroll
