@@ -491,7 +491,7 @@ std::vector<float2> fft_dc_twiddles(int ny, int nz) {
 namespace {
 
 // Compile-time instances for the hot plane shapes; every other factorable shape uses the
-// run-time kernel.  Thread counts divide every pass's task count.
+// run-time kernel.  The pass loops stride by the thread count, so any count is correct.
 struct FftKernelChoice {
   void (*kern)(FftDcArgs);
   int nt, y1, y2, z1, z2;
@@ -499,10 +499,11 @@ struct FftKernelChoice {
 
 FftKernelChoice choose_fft(int ny, int nz) {
   FftKernelChoice c;
-  // 192 x 96 fills a CTA's shared memory (one CTA per SM): half of the next plane (24 of 48
-  // elements per thread) is prefetched in registers; the smaller planes run several CTAs per
-  // SM, whose loads already overlap each other's compute.
-  if (ny == 192 && nz == 96) c = {fft_dc_fixed_kernel<16, 12, 12, 8, 384, 24>, 384, 16, 12, 12, 8};
+  // 192 x 96 fills a CTA's shared memory (one CTA per SM): 24 warps (the pass loops take the
+  // 1152-task first pass in two rounds), a third of the next plane (8 of 24 elements per
+  // thread) prefetched in registers; the smaller planes run several CTAs per SM, whose loads
+  // already overlap each other's compute.
+  if (ny == 192 && nz == 96) c = {fft_dc_fixed_kernel<16, 12, 12, 8, 768, 8>, 768, 16, 12, 12, 8};
   else if (ny == 96 && nz == 48) c = {fft_dc_fixed_kernel<12, 8, 8, 6, 192, 0>, 192, 12, 8, 8, 6};
   else if (ny == 64 && nz == 64) c = {fft_dc_fixed_kernel<8, 8, 8, 8, 256, 0>, 256, 8, 8, 8, 8};
   else {
