@@ -92,6 +92,32 @@ def test_soft_threshold_batch_matches_oracle(gpu, m, n):
     assert rel_err(got, exp) < 5e-5
 
 
+@pytest.mark.parametrize("m,n,batch", [(216, 61, 1200), (27, 10, 3000)])
+def test_soft_threshold_many_blocks_per_cta(gpu, m, n, batch):
+    """More blocks than resident CTAs, so every kernel of the split path runs several blocks
+    per CTA: the tensor-core Gram with its loads prefetched across block boundaries, the eigen
+    kernel's block queue and the apply kernel.  m = 27 is one 32-row chunk per block (the Gram
+    kernel then keeps three row tables).  Half the blocks are rank-3 signal plus noise (three
+    kept components), half noise only (zero output)."""
+    rng = np.random.default_rng(31)
+    r = 3
+    U = crandn(rng, (batch, m, r))
+    V = crandn(rng, (batch, r, n))
+    on = (rng.random(batch) < 0.5).astype(np.float64)
+    A = np.moveaxis(U @ V, 0, 2) * on[None, None, :] + 0.3 * crandn(rng, (m, n, batch))
+    A = A.astype(np.complex64)
+    s = O.block_singular_values(A)
+    lam = 1.1 * float(max(s[on == 0, 0].max(), s[on == 1, r].max()))   # noise below, signal's 3 above
+    d = DeviceBuffer.from_array(A)
+    L.check(L.lib.llr_soft_threshold_batch_dev(m, n, lam, batch, d.ptr, None))
+    got = d.download(np.empty_like(A, order="F"))
+    exp = O.low_rank_soft(A.astype(np.complex128), lam)
+    err = np.linalg.norm((got - exp).reshape(m * n, batch), axis=0)
+    scale = np.maximum(np.linalg.norm(A.reshape(m * n, batch), axis=0), 1e-30)
+    assert float((err / scale).max()) < 5e-5
+    assert np.count_nonzero(np.abs(got[:, :, on == 0]).max(axis=(0, 1))) == 0   # noise-only blocks: zero
+
+
 def _spectrum_blocks(rng, m, n, sigmas):
     """Blocks C = U diag(sigma) V^H with Haar-like random U (m x n) and V (n x n)."""
     out = np.empty((m, n, len(sigmas)), dtype=np.complex128)
