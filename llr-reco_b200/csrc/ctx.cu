@@ -173,6 +173,17 @@ static BlockSource make_source(llr_ctx* c, const int* explicit_shift, float stor
   return s;
 }
 
+// Inside an iteration whose DC stage is the fused FFT kernel, the prox leaves blocks whose output
+// is zero (every singular value below the threshold) unwritten, and the fused kernel zero-fills
+// them as it loads its planes: their bytes are neither written nor read.  Only the split prox
+// path (warp eigen kernel + apply kernel) reports such blocks, and nothing may read the iterate
+// between the two stages (no wavelet stage).
+static bool defer_zero_blocks(const llr_ctx* c) {
+  return c->fused_fft && !c->wavelet_on && c->cfg.subspace_rank == 0 && c->cfg.eig_solver == 0 &&
+         c->d_gram != nullptr && c->d_blk_ra != nullptr && c->g.nq <= 64 &&
+         (long long)c->gy * c->gz <= 4096;
+}
+
 // One prox pass on d_x.  standalone == true keeps the raw convention (used by single-step
 // entry points); otherwise the output is the FFT input (or the image, if the wavelet runs).
 static int prox_pass(llr_ctx* c, cudaStream_t s, const int* explicit_shift, bool standalone, float* block_stat) {
@@ -202,6 +213,7 @@ static int prox_pass(llr_ctx* c, cudaStream_t s, const int* explicit_shift, bool
     op.blk_ra = c->d_blk_ra;
     op.gram_mode = c->cfg.gram_mode;
     op.err = c->d_err;
+    op.defer_zero = (!standalone && !block_stat && !explicit_shift && defer_zero_blocks(c)) ? 1 : 0;
     LLR_TRY(launch_llr_prox(src, op, s));
   }
   if (block_stat || standalone) return LLR_OK;
@@ -239,8 +251,10 @@ static int n_partials(const llr_ctx* c) { return c->hybrid ? kPartX * c->g.nq : 
 
 // Forward 2-D DFT, DC with residual, inverse 2-D DFT in one kernel; residual finalized.
 static int fused_dc_pass(llr_ctx* c, cudaStream_t s, double* out) {
+  const bool zf = defer_zero_blocks(c);
+  const BlockSource zsrc = make_source(c, nullptr, 1.f);
   LLR_TRY(launch_fft_dc(c->d_x, c->d_yhat, c->d_samp_pos, c->d_samp_off, c->d_fft_tw, c->g, c->d_partials,
-                        c->fft_grid, s));
+                        c->fft_grid, zf ? c->d_blk_ra : nullptr, zf ? &zsrc : nullptr, s));
   return launch_finalize(c->d_partials, c->fft_grid, (double)c->load_scale, out ? nullptr : c->d_hist,
                          out ? 0 : c->hist_cap, out ? nullptr : c->d_iter, out ? 0 : 1, out, s);
 }

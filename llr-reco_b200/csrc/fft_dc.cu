@@ -18,6 +18,7 @@
 
 #include "llr_common.cuh"
 #include "llr_internal.h"
+#include "llr_prox_common.cuh"
 
 namespace llr {
 
@@ -250,7 +251,12 @@ struct FftDcArgs {
   int nx, ny, nz, nq;
   int y1, y2, z1, z2;        // ny = y1 y2, nz = z1 z2
   int pitch;                 // odd row pitch of the shared plane
+  const int* zero_ra;        // optional: per-block kept counts of this iteration's prox; blocks
+                             // with 0 were left unwritten and are zero-filled on load
+  BlockSource zsrc;          // block grid and shift of that prox (when zero_ra is set)
 };
+
+constexpr int kZeroFlagMax = 4096;   // blocks per (x) block slab covered by the zero-fill table
 
 // Passes of one axis with every size a compile-time constant (hot plane shapes).
 template <int DIR, int STEP, int B, int BS, int ES, int N1, int N2, int NT>
@@ -337,8 +343,38 @@ __device__ __forceinline__ void fft_dc_body(const FftDcArgs& a, const Geo& geo) 
   float2* tw = reinterpret_cast<float2*>(smem);
   double* red = reinterpret_cast<double*>(smem + align16b(sizeof(float2) * T.total));
   float2* s = reinterpret_cast<float2*>(smem + align16b(sizeof(float2) * T.total) + 32 * sizeof(double));
+  // zero-fill tables: block column of every y, block row of every z (-1: no block), the shift,
+  // and one flag per block of the current x slab
+  int* zgy = reinterpret_cast<int*>(s + (size_t)P * nz);
+  int* zgz = zgy + ny;
+  int* zsh = zgz + nz;
+  unsigned char* zfl = reinterpret_cast<unsigned char*>(smem + align16b(sizeof(float2) * T.total) +
+                                                        32 * sizeof(double) + sizeof(float2) * (size_t)P * nz +
+                                                        align16b(sizeof(int) * (size_t)(ny + nz + 4)));
+  const bool zf = a.zero_ra != nullptr;
   const int tid = threadIdx.x;
   for (int i = tid; i < T.total; i += blockDim.x) tw[i] = a.twiddle[i];
+  if (zf) {
+    if (tid == 0) block_shift(a.zsrc, zsh);
+    __syncthreads();
+    const BlockSource& zs = a.zsrc;
+    for (int y = tid; y < ny; y += blockDim.x) {
+      int r = (y - zsh[1]) % ny;
+      if (r < 0) r += ny;
+      zgy[y] = r < zs.gy * zs.by ? r / zs.by : -1;
+    }
+    for (int z = tid; z < nz; z += blockDim.x) {
+      int r = (z - zsh[2]) % nz;
+      if (r < 0) r += nz;
+      zgz[z] = r < zs.gz * zs.bz ? r / zs.bz : -1;
+    }
+  }
+  // element (y, z) of the current plane lies in a block whose prox output was left unwritten
+  auto zero_at = [&](int y, int z) {
+    if (!zf) return false;
+    const int by = zgy[y], bz = zgz[z];
+    return by >= 0 && bz >= 0 && zfl[by + a.zsrc.gy * bz] != 0;
+  };
   const long long nyz = (long long)ny * nz;
   const long long planes = (long long)a.nx * a.nq;
   const int dz = (int)blockDim.x / ny, dy = (int)blockDim.x - dz * ny;   // per-stride (z, y) step
@@ -359,12 +395,22 @@ __device__ __forceinline__ void fft_dc_body(const FftDcArgs& a, const Geo& geo) 
     const int q = (int)(pl / a.nx), ix = (int)(pl - (long long)q * a.nx);
     float2* g = a.u + pl * nyz;
     __syncthreads();   // previous plane stored, twiddles visible
+    if (zf) {          // flags of the blocks of this plane's x slab
+      const BlockSource& zs = a.zsrc;
+      int r = (ix - zsh[0]) % a.nx;
+      if (r < 0) r += a.nx;
+      const int gxi = r < zs.gx * zs.bx ? r / zs.bx : -1;
+      const int nslab = zs.gy * zs.gz;
+      for (int t = tid; t < nslab; t += blockDim.x)
+        zfl[t] = gxi >= 0 && a.zero_ra[t + (long long)nslab * gxi] == 0;
+      __syncthreads();
+    }
     {   // asynchronous 8-byte copies for what the registers do not hold: all in flight at once
       int z = tid / ny, y = tid - (tid / ny) * ny;
       if constexpr (EPT > 0) {
 #pragma unroll
         for (int i = 0; i < EPT; ++i) {
-          s[z * P + y] = nxt[i];
+          s[z * P + y] = zero_at(y, z) ? make_float2(0.f, 0.f) : nxt[i];
           y += dy;
           z += dz;
           if (y >= ny) { y -= ny; ++z; }
@@ -372,7 +418,10 @@ __device__ __forceinline__ void fft_dc_body(const FftDcArgs& a, const Geo& geo) 
       }
       for (int e = tid + EPT * (int)blockDim.x; e < ny * nz; e += blockDim.x) {
         const unsigned dst = (unsigned)__cvta_generic_to_shared(s + z * P + y);
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(g + e) : "memory");
+        if (zero_at(y, z))
+          s[z * P + y] = make_float2(0.f, 0.f);
+        else
+          asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(g + e) : "memory");
         y += dy;
         z += dz;
         if (y >= ny) { y -= ny; ++z; }
@@ -458,7 +507,8 @@ bool split_len(int n, int& n1, int& n2) {
 
 size_t fft_dc_smem(int ny, int nz, int pitch) {
   const FftTab T = fft_tab(ny, nz);
-  return align16b(sizeof(float2) * T.total) + 32 * sizeof(double) + sizeof(float2) * (size_t)pitch * nz;
+  return align16b(sizeof(float2) * T.total) + 32 * sizeof(double) + sizeof(float2) * (size_t)pitch * nz +
+         align16b(sizeof(int) * (size_t)(ny + nz + 4)) + kZeroFlagMax;
 }
 
 }  // namespace
@@ -534,8 +584,15 @@ int fft_dc_grid(int ny, int nz) {
 }
 
 int launch_fft_dc(float2* u, const float2* yhat, const int* pos, const long long* off, const float2* twiddle,
-                  const Geom& g, double* partials, int grid, cudaStream_t s) {
+                  const Geom& g, double* partials, int grid, const int* zero_ra, const BlockSource* zsrc,
+                  cudaStream_t s) {
   FftDcArgs a;
+  a.zero_ra = nullptr;
+  a.zsrc = BlockSource{};
+  if (zero_ra && zsrc && zsrc->kind == 1 && (long long)zsrc->gy * zsrc->gz <= kZeroFlagMax) {
+    a.zero_ra = zero_ra;
+    a.zsrc = *zsrc;
+  }
   a.u = u; a.yhat = yhat; a.pos = pos; a.off = off; a.twiddle = twiddle; a.partials = partials;
   a.nx = g.nx; a.ny = g.ny; a.nz = g.nz; a.nq = g.nq;
   if (!fft_dc_supported(g.ny, g.nz))

@@ -47,6 +47,8 @@ struct ProxOp {
   int* blk_ra;         // split path: kept count per block (+1 int: the eigen kernel's queue)
   int gram_mode;       // 0: 3xTF32 on tensor cores (tcgen05) where 2n <= 128; 1: FP32 FMA
   int* err;            // device flag set when a bounded wait gives up (never expected)
+  int defer_zero = 0;  // 1: the apply kernel leaves blocks with r_a = 0 unwritten; the fused
+                       // FFT that follows in the same iteration zero-fills them as it loads
 };
 
 // Kept eigenvectors per block that the warp eigen kernel hands to the apply kernel.
@@ -63,7 +65,8 @@ bool fft_dc_supported(int ny, int nz);
 std::vector<float2> fft_dc_twiddles(int ny, int nz);
 int fft_dc_grid(int ny, int nz);
 int launch_fft_dc(float2* u, const float2* yhat, const int* pos, const long long* off, const float2* twiddle,
-                  const Geom& g, double* partials, int grid, cudaStream_t s);
+                  const Geom& g, double* partials, int grid, const int* zero_ra, const BlockSource* zsrc,
+                  cudaStream_t s);
 int launch_diff_norm(const float2* a, const float2* b, long long n, double* part_d, double* part_b, int nblocks,
                      cudaStream_t s);
 int launch_llr_eig_warp(const ProxOp& op, long long nblocks, cudaStream_t stream);

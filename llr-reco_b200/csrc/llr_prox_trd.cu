@@ -1024,7 +1024,7 @@ __global__ void __launch_bounds__(kApplyThreads, 3) llr_apply_kernel(BlockSource
   const int sh[3] = {sh_s[0], sh_s[1], sh_s[2]};
   for (long long blk = blockIdx.x; blk < src.nblocks; blk += gridDim.x) {
     const int ra = op.blk_ra[blk];
-    if (ra < 0) continue;   // uniform over the CTA
+    if (ra < 0 || (ra == 0 && op.defer_zero)) continue;   // uniform over the CTA
     const long long base = src.kind == 1 ? 0 : blk * (long long)m * n;
     for (int r = tid; r < m; r += blockDim.x) {
       RowTab rt;
