@@ -370,10 +370,14 @@ __device__ __forceinline__ void fft_dc_body(const FftDcArgs& a, const Geo& geo) 
     }
   }
   // element (y, z) of the current plane lies in a block whose prox output was left unwritten
+  // (the block column of the thread's y is cached: with a thread count that is a multiple of ny,
+  // y never changes along a thread's elements)
+  int zy = -1, zby = -1;
   auto zero_at = [&](int y, int z) {
     if (!zf) return false;
-    const int by = zgy[y], bz = zgz[z];
-    return by >= 0 && bz >= 0 && zfl[by + a.zsrc.gy * bz] != 0;
+    if (y != zy) { zy = y; zby = zgy[y]; }
+    const int bz = zgz[z];
+    return zby >= 0 && bz >= 0 && zfl[zby + a.zsrc.gy * bz] != 0;
   };
   const long long nyz = (long long)ny * nz;
   const long long planes = (long long)a.nx * a.nq;
@@ -550,10 +554,10 @@ struct FftKernelChoice {
 FftKernelChoice choose_fft(int ny, int nz) {
   FftKernelChoice c;
   // 192 x 96 fills a CTA's shared memory (one CTA per SM): 24 warps (the pass loops take the
-  // 1152-task first pass in two rounds), a third of the next plane (8 of 24 elements per
-  // thread) prefetched in registers; the smaller planes run several CTAs per SM, whose loads
-  // already overlap each other's compute.
-  if (ny == 192 && nz == 96) c = {fft_dc_fixed_kernel<16, 12, 12, 8, 768, 8>, 768, 16, 12, 12, 8};
+  // 1152-task first pass in two rounds).  A register prefetch of the next plane paid before the
+  // iteration zero-filled the blocks the prox left unwritten; with that fill it no longer does
+  // (it also loads those blocks' stale bytes), so no instance prefetches.
+  if (ny == 192 && nz == 96) c = {fft_dc_fixed_kernel<16, 12, 12, 8, 768, 0>, 768, 16, 12, 12, 8};
   else if (ny == 96 && nz == 48) c = {fft_dc_fixed_kernel<12, 8, 8, 6, 192, 0>, 192, 12, 8, 8, 6};
   else if (ny == 64 && nz == 64) c = {fft_dc_fixed_kernel<8, 8, 8, 8, 256, 0>, 256, 8, 8, 8, 8};
   else {
