@@ -4,12 +4,14 @@
 // P = D^T D (2n x 2n) gives G = C^H C as
 //   Re G[i][j] = P[i][j] + P[n+i][n+j],   Im G[i][j] = P[i][n+j] - P[n+i][j].
 // P is one 128 x 128 UMMA accumulator in tensor memory (2n <= 128), K = the m voxel rows.
-// Both operands are the same shared-memory tile of D in the K-major, no-swizzle canonical
-// layout (8-row x 16-byte core matrices), so A = B and the MMA computes D^T D directly.
+// Both operands are the same shared-memory tile of D in the K-major layout with the 128-byte
+// swizzle (one 128-byte row of 32 TF32 per column of D and chunk), so A = B and the MMA
+// computes D^T D directly.
 // Precision: 3xTF32 -- x = hi + lo with hi = tf32(x), and P accumulates hi*hi + hi*lo + lo*hi
 // in FP32, which keeps FP32-level accuracy (the lo*lo term is below FP32 rounding).
-// Rows stream in 32-row chunks, double-buffered: while the tensor core consumes one chunk the
-// 128 threads gather, phase-correct and split the next one.  One elected thread issues the
+// Rows stream in 32-row chunks, double-buffered, with the loads of the chunk two positions
+// ahead (possibly of the CTA's next block) in flight: while the tensor core consumes one chunk
+// the 8 warps gather, phase-correct and split the next one.  One elected thread issues the
 // MMAs and commits them to an mbarrier; every wait is bounded and reports a timeout through
 // op.err instead of hanging.
 #include <cstdio>
