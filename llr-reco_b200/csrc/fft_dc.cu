@@ -287,7 +287,6 @@ __device__ __forceinline__ void axis_pass_fixed(float2* s, const float2* wN) {
 
 // Plane geometry with run-time sizes (any shape split_len accepts).
 struct GeoRt {
-  static constexpr int EPT = 0;   // no register prefetch
   int ny, nz, y1, y2, z1, z2, P;
   __device__ void forward(float2* s, const float2* tw, const FftTab& T) const {
     axis_dispatch<1, 0>(s, nz, P, 1, y1, y2, tw + T.off_y, ny, tw, T);
@@ -310,10 +309,9 @@ struct GeoRt {
 };
 
 // Plane geometry with compile-time sizes: ny = Y1 Y2, nz = Z1 Z2, NT threads.
-template <int Y1, int Y2, int Z1, int Z2, int NT, int PF>
+template <int Y1, int Y2, int Z1, int Z2, int NT>
 struct GeoFixed {
   static constexpr int NY = Y1 * Y2, NZ = Z1 * Z2, PP = NY | 1;
-  static constexpr int EPT = PF;   // elements per thread of the next plane prefetched in registers
   int ny = NY, nz = NZ, y1 = Y1, y2 = Y2, z1 = Z1, z2 = Z2, P = PP;
   __device__ void forward(float2* s, const float2* tw, const FftTab& T) const {
     axis_pass_fixed<1, 0, NZ, PP, 1, Y1, Y2, NT>(s, tw + T.off_y);
@@ -383,18 +381,6 @@ __device__ __forceinline__ void fft_dc_body(const FftDcArgs& a, const Geo& geo) 
   const long long planes = (long long)a.nx * a.nq;
   const int dz = (int)blockDim.x / ny, dy = (int)blockDim.x - dz * ny;   // per-stride (z, y) step
   double err = 0.0;
-  // Fixed shapes with one CTA per SM: the first EPT elements per thread of the next plane are
-  // loaded into registers (coalesced) while this plane is transformed, so that part of the
-  // HBM latency and transfer hides behind the compute; the rest arrives by cp.async.
-  constexpr int EPT = Geo::EPT;
-  float2 nxt[EPT > 0 ? EPT : 1];
-  if constexpr (EPT > 0) {
-    if ((long long)blockIdx.x < planes) {
-      const float2* gn = a.u + (long long)blockIdx.x * nyz;
-#pragma unroll
-      for (int i = 0; i < EPT; ++i) nxt[i] = gn[tid + i * (int)blockDim.x];
-    }
-  }
   for (long long pl = blockIdx.x; pl < planes; pl += gridDim.x) {
     const int q = (int)(pl / a.nx), ix = (int)(pl - (long long)q * a.nx);
     float2* g = a.u + pl * nyz;
@@ -409,18 +395,9 @@ __device__ __forceinline__ void fft_dc_body(const FftDcArgs& a, const Geo& geo) 
         zfl[t] = gxi >= 0 && a.zero_ra[t + (long long)nslab * gxi] == 0;
       __syncthreads();
     }
-    {   // asynchronous 8-byte copies for what the registers do not hold: all in flight at once
+    {   // asynchronous 8-byte copies: every element in flight at once, no register staging
       int z = tid / ny, y = tid - (tid / ny) * ny;
-      if constexpr (EPT > 0) {
-#pragma unroll
-        for (int i = 0; i < EPT; ++i) {
-          s[z * P + y] = zero_at(y, z) ? make_float2(0.f, 0.f) : nxt[i];
-          y += dy;
-          z += dz;
-          if (y >= ny) { y -= ny; ++z; }
-        }
-      }
-      for (int e = tid + EPT * (int)blockDim.x; e < ny * nz; e += blockDim.x) {
+      for (int e = tid; e < ny * nz; e += blockDim.x) {
         const unsigned dst = (unsigned)__cvta_generic_to_shared(s + z * P + y);
         if (zero_at(y, z))
           s[z * P + y] = make_float2(0.f, 0.f);
@@ -431,14 +408,6 @@ __device__ __forceinline__ void fft_dc_body(const FftDcArgs& a, const Geo& geo) 
         if (y >= ny) { y -= ny; ++z; }
       }
       asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
-      if constexpr (EPT > 0) {
-        const long long pn = pl + gridDim.x;
-        if (pn < planes) {
-          const float2* gn = a.u + pn * nyz;
-#pragma unroll
-          for (int i = 0; i < EPT; ++i) nxt[i] = gn[tid + i * (int)blockDim.x];
-        }
-      }
     }
     __syncthreads();
     // forward: y axis (rows, element stride 1, batch stride P), then z axis (columns)
@@ -492,9 +461,9 @@ __global__ void __launch_bounds__(kFftThreads, 1) fft_dc_kernel(FftDcArgs a) {
   fft_dc_body(a, geo);
 }
 
-template <int Y1, int Y2, int Z1, int Z2, int NT, int PF>
+template <int Y1, int Y2, int Z1, int Z2, int NT>
 __global__ void __launch_bounds__(NT, 1) fft_dc_fixed_kernel(FftDcArgs a) {
-  fft_dc_body(a, GeoFixed<Y1, Y2, Z1, Z2, NT, PF>());
+  fft_dc_body(a, GeoFixed<Y1, Y2, Z1, Z2, NT>());
 }
 
 bool split_len(int n, int& n1, int& n2) {
@@ -554,12 +523,10 @@ struct FftKernelChoice {
 FftKernelChoice choose_fft(int ny, int nz) {
   FftKernelChoice c;
   // 192 x 96 fills a CTA's shared memory (one CTA per SM): 24 warps (the pass loops take the
-  // 1152-task first pass in two rounds).  A register prefetch of the next plane paid before the
-  // iteration zero-filled the blocks the prox left unwritten; with that fill it no longer does
-  // (it also loads those blocks' stale bytes), so no instance prefetches.
-  if (ny == 192 && nz == 96) c = {fft_dc_fixed_kernel<16, 12, 12, 8, 768, 0>, 768, 16, 12, 12, 8};
-  else if (ny == 96 && nz == 48) c = {fft_dc_fixed_kernel<12, 8, 8, 6, 192, 0>, 192, 12, 8, 8, 6};
-  else if (ny == 64 && nz == 64) c = {fft_dc_fixed_kernel<8, 8, 8, 8, 256, 0>, 256, 8, 8, 8, 8};
+  // 1152-task first pass in two rounds); the smaller planes run several CTAs per SM.
+  if (ny == 192 && nz == 96) c = {fft_dc_fixed_kernel<16, 12, 12, 8, 768>, 768, 16, 12, 12, 8};
+  else if (ny == 96 && nz == 48) c = {fft_dc_fixed_kernel<12, 8, 8, 6, 192>, 192, 12, 8, 8, 6};
+  else if (ny == 64 && nz == 64) c = {fft_dc_fixed_kernel<8, 8, 8, 8, 256>, 256, 8, 8, 8, 8};
   else {
     c.kern = fft_dc_kernel;
     c.nt = kFftThreads;
