@@ -1,5 +1,5 @@
 """CPU checks of the CNN oracle: its analytic gradients against finite differences, BF16
-rounding, and the subspace channel packing (the oracle itself, before it judges the GPU)."""
+rounding, and the subspace channel packing (the oracle itself, before it is used to check the GPU)."""
 import numpy as np
 import pytest
 
