@@ -134,13 +134,55 @@ def measured_peaks() -> dict:
     return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
-def profiled_traffic(kernel: str, config: str) -> float | None:
-    """DRAM bytes per launch of ``kernel`` recorded from an ncu capture in profiles/."""
-    p = os.path.join(ROOT, "profiles", f"{kernel}_{config}.md")
+def profiled_traffic(kernel: str, config: str) -> dict | None:
+    """DRAM bytes per launch of ``kernel`` at ``config``, as ``--ncu-traffic`` wrote them from an
+    ncu capture into profiles/<kernel>_<config>.json (None when no capture was recorded)."""
+    p = os.path.join(ROOT, "profiles", f"{kernel}_{config}.json")
     if not os.path.exists(p):
         return None
-    m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(p).read())
-    return float(m.group(1)) if m else None
+    with open(p) as f:
+        return json.load(f)
+
+
+def _ncu_bytes(value: str, unit: str) -> float:
+    scale = {"byte": 1.0, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9, "Tbyte": 1e12,
+             "KB": 1e3, "MB": 1e6, "GB": 1e9, "B": 1.0}
+    return float(value.replace(",", "")) * scale.get(unit.strip(), 1.0)
+
+
+def write_traffic(args) -> None:
+    """Sum dram__bytes_read.sum + dram__bytes_write.sum per launch of the kernels matching
+    ``--traffic-kernels`` from ``ncu -i <rep> --page raw --csv`` output, scale by
+    ``--traffic-scale`` (units processed at the target size / units in the capture) and write
+    profiles/<--traffic-name>_<--config>.json."""
+    import csv
+    with open(args.ncu_traffic) as f:
+        rows = [r for r in csv.reader(f) if r]
+    head = rows[0]
+    units = rows[1]
+    ik, ir, iw = head.index("Kernel Name"), head.index("dram__bytes_read.sum"), head.index("dram__bytes_write.sum")
+    pat = re.compile(args.traffic_kernels)
+    per_kernel: dict[str, list[float]] = {}
+    for r in rows[2:]:
+        name = r[ik]
+        if not pat.search(name):
+            continue
+        short = re.sub(r"\(.*", "", name).split("::")[-1]
+        per_kernel.setdefault(short, []).append(_ncu_bytes(r[ir], units[ir]) + _ncu_bytes(r[iw], units[iw]))
+    if not per_kernel:
+        raise SystemExit(f"no kernel matching {args.traffic_kernels!r} in {args.ncu_traffic}")
+    mean = {k: sum(v) / len(v) for k, v in per_kernel.items()}
+    out = {"kernel": args.traffic_name, "config": args.config,
+           "captured_on": args.traffic_captured_on or args.config, "scale": args.traffic_scale,
+           "per_kernel_captured_bytes": {k: round(v, 1) for k, v in mean.items()},
+           "launches_averaged": {k: len(v) for k, v in per_kernel.items()},
+           "dram_bytes_per_launch": sum(mean.values()) * args.traffic_scale,
+           "source": f"dram__bytes_read.sum + dram__bytes_write.sum from {os.path.basename(args.ncu_traffic)}"}
+    path = os.path.join(ROOT, "profiles", f"{args.traffic_name}_{args.config}.json")
+    with open(path, "w") as f:
+        json.dump(out, f, indent=1)
+        f.write("\n")
+    print(json.dumps(out))
 
 
 # ---------------------------------------------------------------------------------------
@@ -168,11 +210,10 @@ def gpu_forward(x: np.ndarray) -> np.ndarray:
 def make_data(name: str, seed: int, use_gpu: bool):
     """Seeded phantom k-space; the b-table is the shared acquisition protocol of the learned
     warm start (so its temporal subspace is the one the network was trained in)."""
-    from llr_b200.phantom import make_dataset
-    from llr_b200.warmstart import Protocol
+    from llr_b200.phantom import PROTOCOL_SEED, make_dataset
     c = config_workload(name)
     return c, make_dataset(c["vol"], c["shells"], c["accel"], seed, centre=16,
-                           forward=gpu_forward if use_gpu else None, protocol_seed=Protocol().protocol_seed)
+                           forward=gpu_forward if use_gpu else None, protocol_seed=PROTOCOL_SEED)
 
 
 def warm_start_headline(args, c, d) -> dict:
@@ -212,6 +253,18 @@ def warm_start_headline(args, c, d) -> dict:
         if p is not None and l is not None:
             out[key]["speedup"] = round(p[1] / (l[1] + net_ms), 3)
     return out
+
+
+def bench_config(name: str, c: dict, nq: int, world: int) -> dict:
+    """The ``config`` object both arms print (identical for the same --config and N)."""
+    nx, ny, nz = c["vol"]
+    E = nx * ny * nz * nq
+    return {"workload": workload_label(name, c, nq), "vol": list(c["vol"]), "nq": nq, "block": list(c["block"]),
+            "accel": c["accel"], "lambda_rule": "0.02 x largest block singular value of the zero-filled image, shift 0",
+            "l2": f"no flush: the {8 * E / 1e9:.2f} GB iterate exceeds the 126 MB L2" if 8 * E > 126e6 else
+                  f"flushed: a 512 MB buffer is written before every timed iteration (the {8 * E / 1e6:.1f} MB "
+                  f"iterate fits the 126 MB L2)",
+            "parallelism": f"replicas x{world}"}
 
 
 def workload_label(name: str, c: dict, nq: int) -> str:
@@ -257,12 +310,26 @@ def run_b200(args, dist: Dist) -> None:
     ctx.set_lambda(0.02 * sigma)
     x0 = ctx.download_image() if (dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline) else None
 
-    # warm-up, then the timed region: K iterations, per-stage CUDA events on the context stream
+    # warm-up, then the timed region: K iterations, per-stage CUDA events on the context stream.
+    # An iterate that fits the 126 MB L2 is evicted before every timed iteration by writing a
+    # 512 MB buffer (outside the events), so no iteration starts with its input in L2.
+    flush = None
+    if 8 * E <= 126e6:
+        import torch
+        flush = torch.empty(128 << 20, dtype=torch.float32, device=f"cuda:{dev}")
     ctx.iterate_profiled(max(args.warmup, 1))
     dist.barrier()
     clocks = ClockSampler(dev)
     clocks.start()
-    stage_ms, total_ms = ctx.iterate_profiled(args.steps)
+    if flush is None:
+        stage_ms, total_ms = ctx.iterate_profiled(args.steps)
+    else:
+        stage_ms, total_ms = np.zeros(5), 0.0
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize(dev)
+            st, tt = ctx.iterate_profiled(1)
+            stage_ms, total_ms = stage_ms + st, total_ms + tt
     clk = clocks.stop()
     dist.barrier()
     t_max = dist.max(total_ms)
@@ -278,14 +345,17 @@ def run_b200(args, dist: Dist) -> None:
     prox_bytes = 16.0 * E
     peaks = measured_peaks()
     achieved = prox_bytes / (per_launch_ms["llr_prox"] / 1e3) / 1e9
-    traffic = profiled_traffic("llr_prox", args.config)
+    prof = profiled_traffic("llr_prox", args.config)
     it_bytes = 16.0 * E * 3 + 24.0 * E / c["accel"]
     prox_label = ("LLR prox stage: llr_subspace_kernel (X <- LR(X S) S^H)" if "srank" in c else
                   "LLR prox stage: llr_gram_tc_kernel + llr_eig_warp_kernel + llr_apply_kernel")
     roofline = {"bound": "hbm", "kernel": prox_label,
                 "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "peak_source": peaks["source"],
                 "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4),
-                "algorithmic_bytes_per_launch": prox_bytes, "traffic": traffic,
+                "algorithmic_bytes_per_launch": prox_bytes,
+                "traffic": None if prof is None else prof["dram_bytes_per_launch"],
+                "traffic_source": None if prof is None else
+                f"profiles/llr_prox_{args.config}.json (captured on {prof['captured_on']}, x{prof['scale']:g})",
                 "stage_ms_per_iteration": {k: round(v, 4) for k, v in per_launch_ms.items()},
                 "iteration_algorithmic_bytes": it_bytes,
                 "iteration_hbm_frac": round(it_bytes / (t_max / args.steps / 1e3) / 1e9 / peaks["hbm_gbs"], 4)}
@@ -314,7 +384,7 @@ def run_b200(args, dist: Dist) -> None:
 
     # learned + mixed against plain FP32: time to NRMSE <= 1e-3 (rank 0, N = 1)
     headline = None
-    if dist.rank == 0 and dist.world == 1 and not args.no_warm_start:
+    if dist.rank == 0 and dist.world == 1 and not args.no_warm_start and args.config == "c2":
         try:
             headline = warm_start_headline(args, c, d)
         except Exception as e:  # reported, never fatal to the throughput measurement
@@ -338,11 +408,9 @@ def run_b200(args, dist: Dist) -> None:
             "warmup": args.warmup, "ms_per_step": round(t_max / args.steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "complex64 (FP32)",
             "data": "synthetic (seeded ellipsoid DTI phantom, VD mask, SNR 30 noise)",
-            "config": {"workload": workload_label(args.config, c, nq), "vol": list(c["vol"]), "nq": nq,
-                       "block": list(c["block"]), "accel": c["accel"], "measured_undersampling":
-                           round(ctx.measurement_stats()[1], 3), "lambda": 0.02 * sigma,
-                       "l2": f"no flush: the {8 * E / 1e9:.2f} GB iterate exceeds the 126 MB L2", "parallelism": f"replicas x{dist.world}",
-                       "path": "hybrid (x-transform eliminated)"},
+            "config": bench_config(args.config, c, nq, dist.world),
+            "lambda": 0.02 * sigma, "measured_undersampling": round(ctx.measurement_stats()[1], 3),
+            "path": "hybrid (x-transform eliminated: line-structured sampling)",
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "warm_start": headline,
             "gpu_launches": n_kernels * args.steps,
             "residual_first_last": [float(hist[0]), float(hist[-1])],
@@ -352,15 +420,17 @@ def run_b200(args, dist: Dist) -> None:
 
 
 def run_reference(args, dist: Dist) -> None:
+    """The reference's CPU path (FP32 numpy/scipy restatement, all host threads) on the same
+    seeded data and threshold rule as the B200 arm.  Imports nothing that maps libllr_b200.so."""
     if dist.rank != 0:
         return
-    from oracle.cpu_baseline import time_iteration_sample
-    from llr_b200.phantom import make_dataset, centred_fft_unitary
+    from oracle.cpu_baseline import sigma_max_all_blocks, time_iteration_sample
+    from llr_b200.phantom import PROTOCOL_SEED, make_dataset, centred_fft_unitary
     from threadpoolctl import threadpool_limits
     from oracle import llr_oracle as O
     c = config_workload(args.config)
     d = make_dataset(c["vol"], c["shells"], c["accel"], args.seed, centre=16, mask_fn=O.vd_mask,
-                     forward=centred_fft_unitary)
+                     forward=centred_fft_unitary, protocol_seed=PROTOCOL_SEED)
     nq = d.y.shape[3]
     # zero-filled start A^H y with the CPU restatement
     import scipy.fft as sf
@@ -371,12 +441,9 @@ def run_reference(args, dist: Dist) -> None:
     for q in range(nq):
         x0[..., q] = sf.ifftn(d.y[..., q] * pre, norm="ortho", workers=-1) * np.conj(pre)
     bs = c["block"]
-    nb = int(np.prod(O.grid_dim(c["vol"], bs)))
-    s_sample = O.block_singular_values(O.lift_data_set(x0[..., :].copy(order="F"), bs, (0, 0, 0), 0,
-                                                       min(nb, 2048)))
-    lam = 0.02 * float(s_sample[:, 0].max())
-    times = []
     with threadpool_limits(1):
+        lam = 0.02 * sigma_max_all_blocks(x0, bs)
+        times = []
         for i in range(args.warmup + args.steps):
             r = time_iteration_sample(x0, d.y, bs, "soft", 0, lam, n_blocks=args.cpu_blocks, n_vols=args.cpu_vols,
                                       seed=args.seed + i)
@@ -389,8 +456,8 @@ def run_reference(args, dist: Dist) -> None:
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(sec * 1e3, 2), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "complex64 (FP32)",
         "data": "synthetic (seeded ellipsoid DTI phantom, VD mask, SNR 30 noise)",
-        "config": {"workload": workload_label(args.config, c, nq), "vol": list(c["vol"]), "nq": nq,
-                   "block": list(bs), "accel": c["accel"], "parallelism": "host threads"},
+        "config": bench_config(args.config, c, nq, dist.world),
+        "lambda": lam,
         "cpu_baseline": {"value": round(value, 5), "unit": UNIT, "cores": r["threads"], "kind": "port",
                          "sample": r["sample"] + "; the reference (Rust + unvendored git crates) cannot be built "
                                                  "here, so its algorithm is restated in numpy/scipy"},
@@ -420,7 +487,17 @@ def main(argv=None):
                     help="0: fused per-plane FFT + DC + inverse FFT kernel; 1: cuFFT passes")
     ap.add_argument("--eig-solver", type=int, default=0,
                     help="0: tridiagonal, warp per block; 1: Jacobi; 2: tridiagonal, CTA per block")
+    ap.add_argument("--ncu-traffic", metavar="CSV",
+                    help="write profiles/<--traffic-name>_<--config>.json from `ncu -i REP --page raw --csv` output "
+                         "and exit")
+    ap.add_argument("--traffic-name", default="llr_prox")
+    ap.add_argument("--traffic-kernels", default="llr_gram_tc|llr_eig_warp|llr_apply")
+    ap.add_argument("--traffic-scale", type=float, default=1.0)
+    ap.add_argument("--traffic-captured-on", default=None)
     args = ap.parse_args(argv)
+    if args.ncu_traffic:
+        write_traffic(args)
+        return
     if args.warmup < 3:
         print("note: warm-up raised to 3 (timing rules)", file=sys.stderr)
         args.warmup = 3

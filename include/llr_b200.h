@@ -179,12 +179,16 @@ int llr_low_rank_batch_dev(int32_t m, int32_t n, int32_t rank, int32_t batch,
  * allocate device memory (a caller replaying its own CUDA graph under a fixed memory plan,
  * a device whose memory belongs to another framework's pool, a loop that must not pay an
  * allocator call per invocation).  No counterpart in the reference.  It allocates nothing:
- * its scratch is a static 256 KiB device array per GPU (held until exit), so batch must be
- * <= 65536 (LLR_ERR_INVALID otherwise).  The first call on a device looks up that array's
- * device address; make that first call before any stream capture.  All calls on a GPU
- * share the array and it keeps the last call's contents (the count word is cleared by every
- * call), so calls that can run at the same time on one GPU, e.g. on two streams, race:
- * serialise them. */
+ * it runs the fused tridiagonal prox kernel (no per-matrix Gram scratch; the allocating call
+ * runs the split Gram / eigen / apply kernels, so the two agree to the prox tolerance,
+ * relative 5e-5, not bitwise), and the list of matrices keeping more than 16 components,
+ * which the Jacobi kernel finishes, lives in a static 256 KiB device array per GPU (held
+ * until exit), so batch must be <= 65536 (LLR_ERR_INVALID otherwise).  The first call on a
+ * device looks up that array's device address and caches it; make that first call before
+ * any stream capture, and do not use this entry point on a device after cudaDeviceReset().
+ * All calls on a GPU share the array and it keeps the last call's contents (the count word
+ * is cleared by every call), so calls that can run at the same time on one GPU, e.g. on two
+ * streams, race: serialise them. */
 int llr_low_rank_batch_dev_noalloc(int32_t m, int32_t n, int32_t rank, int32_t batch,
                                    llr_cf32* d_mats, void* stream);
 /* Singular-value soft threshold of every (m, n) matrix, n <= 64. */

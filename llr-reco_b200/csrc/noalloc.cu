@@ -1,13 +1,17 @@
 // Allocation-free variant of the batched hard-rank prox.
 //
-// llr_low_rank_batch_dev() allocates a small block list (batch + 1 ints) with
-// cudaMallocAsync on every call: the tridiagonal-path kernel appends to it the matrices that
-// the Jacobi kernel must finish.  Some callers cannot let the library allocate: a host that
-// records the call into a CUDA graph it owns and replays it under a fixed memory plan, a
-// process whose device memory is handed out by another framework's pool, or a real-time
-// loop that must not pay an allocator call per invocation.  For them this entry point takes
-// the list from a file-scope device array instead, so it calls no cudaMalloc, cudaFree or
-// allocating library routine.
+// llr_low_rank_batch_dev() allocates, with cudaMallocAsync on every call, a per-matrix packed
+// Gram buffer and 2 * batch + 2 ints (fallback list and count, kept counts and a queue
+// counter), and takes the split path: tensor-core Gram kernel, warp eigen kernel, apply
+// kernel.  Some callers cannot let the library allocate: a host that records the call into a
+// CUDA graph it owns and replays it under a fixed memory plan, a process whose device memory is
+// handed out by another framework's pool, or a real-time loop that must not pay an allocator
+// call per invocation.  For them this entry point runs the fused tridiagonal prox kernel, which
+// needs no per-matrix scratch, and takes its one piece of scratch -- the list of matrices that
+// keep more components than the fused kernel handles (more than 16), finished by the Jacobi
+// kernel -- from a file-scope device array.  It calls no cudaMalloc, cudaFree or allocating
+// library routine.  The two entry points compute the same operation with different kernels;
+// their outputs agree to the low-rank prox tolerance (relative 5e-5 on well-separated spectra).
 #include <cstring>
 #include <mutex>
 
@@ -28,7 +32,10 @@ std::mutex g_noalloc_mu;
 int* g_noalloc_addr[kMaxDevices] = {nullptr};
 
 // The array's name is only a host-side stand-in in host code; the device address must be
-// queried once per device, with that device current.
+// queried once per device, with that device current.  The cached address belongs to the
+// device's primary context: after cudaDeviceReset() on a device the module is loaded again and
+// the cache entry for that device is stale, so this entry point must not be used on a device
+// that was reset during the process's life.
 int noalloc_scratch(int** out) {
   int dev = 0;
   LLR_CUDA_TRY(cudaGetDevice(&dev));

@@ -152,6 +152,10 @@ def make_dataset(vol, shells, accel, seed, centre=16, snr=30.0, n_ellipsoids=6,
     return Dataset(x_true=x, mask=mask, b=b, g=g, noise_sigma=sigma, y=np.asfortranarray(k.astype(np.complex64)))
 
 
+# Seed of the b-table every benchmark subject shares (the acquisition protocol the learned warm
+# start was trained in); phantom, mask and noise come from the subject's own seed.
+PROTOCOL_SEED = 1234
+
 # Configurations of the benchmark suite (shapes and acquisition parameters).
 CONFIGS = {
     "c1": dict(vol=(64, 64, 64), shells=[(0, 1), (1000, 16)], accel=4.0, block=(8, 8, 8), n_iter=50),

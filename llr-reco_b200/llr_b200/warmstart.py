@@ -25,7 +25,7 @@ from ._lib import check, lib
 from ._lib import LLR_PROX_SOFT_THRESH
 from .api import DeviceBuffer, ReconContext, ReconParams
 from .cnn import Cnn, DeviceArray, subspace_channels_dev, subspace_image_dev
-from .phantom import b_table, dti_subspace, make_dataset
+from .phantom import PROTOCOL_SEED, b_table, dti_subspace, make_dataset
 
 
 @dataclass
@@ -38,7 +38,7 @@ class Protocol:
     centre: int = 12
     lam_rel: float = 0.02
     srank: int = 7
-    protocol_seed: int = 1234
+    protocol_seed: int = PROTOCOL_SEED
     recon_seed: int = 3
     fixed_partition: bool = True
     gram_mode: int = 0

@@ -76,6 +76,28 @@ def signal_dc(x: np.ndarray, y: np.ndarray, threads: int) -> float:
     return err
 
 
+def sigma_max_all_blocks(x: np.ndarray, block_size, shift=(0, 0, 0), batch: int = 512,
+                         threads: int | None = None) -> float:
+    """Largest singular value over every block of ``x`` at ``shift`` (lift_data_set order,
+    block.rs:147-164), from the FP64 Gram matrix of each Casorati block (eigvalsh), in batches
+    over host threads.  The threshold rule lambda = 0.02 sigma_max uses it."""
+    threads = threads or _threads()
+    nx, ny, nz, nq = x.shape
+    vol = (nx, ny, nz)
+    total = int(np.prod(O.grid_dim(vol, block_size)))
+    flat = x.reshape(nx * ny * nz, nq, order="F")
+
+    def work(b0):
+        ids = [O._block_voxel_index(vol, block_size, O.block_coord(b, vol, block_size, shift))
+               for b in range(b0, min(b0 + batch, total))]
+        mats = np.stack([flat[v, :] for v in ids], axis=0).astype(np.complex128)
+        G = np.conj(np.swapaxes(mats, 1, 2)) @ mats
+        return float(np.sqrt(max(np.linalg.eigvalsh(G)[:, -1].max(), 0.0)))
+
+    with ThreadPoolExecutor(threads) as ex:
+        return max(ex.map(work, range(0, total, batch)))
+
+
 def time_iteration_sample(x: np.ndarray, y: np.ndarray, block_size, mode: str, rank: int, lam: float,
                           n_blocks: int, n_vols: int, seed: int = 0, threads: int | None = None) -> dict:
     """Time ``n_blocks`` blocks of the prox and ``n_vols`` volumes of A/DC/A^H; scale to one

@@ -13,6 +13,7 @@ import pytest
 from conftest import crandn, rel_err
 
 from llr_b200 import DeviceBuffer, _lib as L
+from oracle import llr_oracle as O
 
 pytestmark = pytest.mark.gpu
 
@@ -40,6 +41,25 @@ def test_noalloc_matches_allocating_entry_point_on_two_calls(gpu, m, n, rank):
         got = d_new.download(np.empty_like(A, order="F"))
         assert np.all(np.isfinite(got))
         assert rel_err(got, ref) <= TOL, (call, rel_err(got, ref))
+
+
+@pytest.mark.parametrize("m,n,rank", [(216, 61, 20), (64, 40, 24)])
+def test_noalloc_static_list_path_on_two_calls(gpu, m, n, rank):
+    """Ranks above 16 send every matrix through the static list to the Jacobi kernel: the list
+    is filled, read and its count cleared again on the second call (different batch size)."""
+    rng = np.random.default_rng(47)
+    for call, batch in enumerate((37, 23)):
+        A = _batch(rng, m, n, rank, batch)
+        d_ref, d_new = DeviceBuffer.from_array(A), DeviceBuffer.from_array(A)
+        L.check(L.lib.llr_low_rank_batch_dev(m, n, rank, batch, d_ref.ptr, None))
+        L.check(L.lib.llr_low_rank_batch_dev_noalloc(m, n, rank, batch, d_new.ptr, None))
+        L.check(L.lib.llr_stream_sync(None))
+        ref = d_ref.download(np.empty_like(A, order="F"))
+        got = d_new.download(np.empty_like(A, order="F"))
+        exact = O.low_rank_hard(A.astype(np.complex128), rank)
+        assert np.all(np.isfinite(got))
+        assert rel_err(got, ref) <= TOL, (call, rel_err(got, ref))
+        assert rel_err(got, exact) <= TOL, (call, rel_err(got, exact))
 
 
 def test_noalloc_rejects_batches_beyond_its_static_list(gpu):
