@@ -217,6 +217,19 @@ int llr_idwt3_axis_dev(llr_cf32* d_vol, const llr_cf32* d_decomp, const uint32_t
                        const uint32_t decomp_size[3], uint32_t axis, uint32_t filter_len,
                        const float* d_lo_r, const float* d_hi_r, const int32_t shift[3],
                        void* stream);
+/* The reference's native DWT launchers with their exact C signatures, as cudwt3.rs:97-100
+ * binds them (kernels.cu:273-310 dwt3_axis, kernels.cu:312-348 idwt3_axis): vol_size and
+ * decomp_size are HOST arrays of 3 (x fastest); vol_data, decomp, the filters and rand_shift
+ * (3 ints) are DEVICE pointers.  Default stream; the call synchronises and returns a
+ * cudaError_t (0 = success; cudaErrorInvalidValue for a bad argument).  dwt3_axis writes the
+ * approximation (first sub_band_size(n, filter_len) coefficients) then the detail along
+ * `axis`; idwt3_axis keeps the centre vol_size[axis] samples.  The circular shift wraps each
+ * axis by its own extent (kernels.cu:80-95 wraps all three by vol_size[0]; equal when the
+ * shift is zero). */
+int dwt3_axis(llr_cf32* vol_data, llr_cf32* decomp, unsigned int* vol_size, unsigned int* decomp_size,
+              unsigned int axis, unsigned int filter_len, float* lo_d, float* hi_d, int* rand_shift);
+int idwt3_axis(llr_cf32* vol_data, llr_cf32* decomp, unsigned int* vol_size, unsigned int* decomp_size,
+               unsigned int axis, unsigned int filter_len, float* lo_r, float* hi_r, int* rand_shift);
 /* wavelet_denoise (lib.rs:430-458) on nvol volumes in place; levels 0 -> max. */
 int llr_wavelet_denoise_dev(llr_cf32* d_vols, const int32_t vol_size[3], int32_t nvol,
                             int32_t moments, int32_t levels, float alpha, void* stream);

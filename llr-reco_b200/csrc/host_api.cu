@@ -102,7 +102,8 @@ int launch_rhs_cdgmm(int m, int n, int batch, float2* a, const float* d, cudaStr
 int launch_cgemm(int m, int k, int n, int batch, int broadcast_a, float2 alpha, float2 beta, int ta, int tb,
                  const float2* A, const float2* B, float2* C, cudaStream_t s);
 int launch_dwt_axis_ref(const float2* vol, float2* dec, const uint32_t* vs, const uint32_t* ds, int axis,
-                        const float* lo, const float* hi, int F, const int* sh, int inverse, cudaStream_t s);
+                        const float* lo, const float* hi, int F, const int* sh, int inverse, cudaStream_t s,
+                        const float* d_lo = nullptr, const float* d_hi = nullptr, const int* d_sh = nullptr);
 int launch_hard_project(float2* x, const float2* y, long long n, double* partials, int nblocks, cudaStream_t s);
 int launch_conj_transpose(const float2* in, float2* out, int m, int n, int batch, cudaStream_t s);
 int launch_finalize(const double* partials, int np, double scale, double* hist, long long cap, long long* it,
@@ -445,6 +446,38 @@ int llr_idwt3_axis_dev(llr_cf32* v, const llr_cf32* d, const uint32_t* vs, const
   LLR_CUDA_TRY(cudaMemcpy(hhi, hi, F * sizeof(float), cudaMemcpyDeviceToHost));
   return launch_dwt_axis_ref((const float2*)v, (float2*)d, vs, ds, (int)axis, hlo, hhi, (int)F, sh, 1,
                              (cudaStream_t)stream);
+}
+
+// The reference's native launchers (kernels.cu:273-348) as its Rust code binds them
+// (cudwt3.rs:97-100): host size arrays, device volume / decomposition / filter / shift
+// pointers, default stream, synchronise, return the cudaError_t.  The circular shift wraps
+// each axis by its own extent.
+static int dwt3_axis_abi(llr_cf32* vol, llr_cf32* dec, const unsigned* vs, const unsigned* ds, unsigned axis,
+                         unsigned F, const float* lo, const float* hi, const int* sh, int inverse) {
+  if (!vol || !dec || !vs || !ds || !lo || !hi || !sh || axis > 2 || F < 2 || F > 20)
+    return (int)cudaErrorInvalidValue;
+  for (int a = 0; a < 3; ++a)
+    if (vs[a] == 0 || ds[a] == 0) return (int)cudaErrorInvalidValue;
+  const unsigned nc = (vs[axis] + F - 1) / 2;
+  if ((!inverse && ds[axis] < 2 * nc) || (inverse && ds[axis] != 2 * nc)) return (int)cudaErrorInvalidValue;
+  for (int a = 0; a < 3; ++a)
+    if (a != (int)axis && vs[a] != ds[a]) return (int)cudaErrorInvalidValue;
+  int st = launch_dwt_axis_ref((const float2*)vol, (float2*)dec, vs, ds, (int)axis, nullptr, nullptr, (int)F, nullptr,
+                               inverse, 0, lo, hi, sh);
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e == cudaSuccess && st != LLR_OK) e = cudaErrorLaunchFailure;
+  return (int)e;
+}
+
+int dwt3_axis(llr_cf32* vol_data, llr_cf32* decomp, unsigned int* vol_size, unsigned int* decomp_size,
+              unsigned int axis, unsigned int filter_len, float* lo_d, float* hi_d, int* rand_shift) {
+  return dwt3_axis_abi(vol_data, decomp, vol_size, decomp_size, axis, filter_len, lo_d, hi_d, rand_shift, 0);
+}
+
+int idwt3_axis(llr_cf32* vol_data, llr_cf32* decomp, unsigned int* vol_size, unsigned int* decomp_size,
+               unsigned int axis, unsigned int filter_len, float* lo_r, float* hi_r, int* rand_shift) {
+  return dwt3_axis_abi(vol_data, decomp, vol_size, decomp_size, axis, filter_len, lo_r, hi_r, rand_shift, 1);
 }
 
 int llr_wavelet_denoise_dev(llr_cf32* d_vols, const int32_t* vs, int32_t nvol, int32_t moments, int32_t levels,

@@ -277,8 +277,29 @@ int wavelet_denoise_strided(const WaveletPlan& p, float2* data, long long sx, lo
 // ---------------------------------------------------------------------------------------
 namespace {
 
+// Taps and shift come from the kernel arguments, or, when d_lo / d_sh are non-null, from
+// device memory (the reference's native interface passes device filter and shift pointers,
+// kernels.cu:155-156, 215-216).
+__device__ __forceinline__ void load_taps_shift(const Taps& t, const float* d_lo, const float* d_hi, const int* d_sh,
+                                                int s0, int s1, int s2, float* lo, float* hi, int* sh) {
+  if (threadIdx.x < (unsigned)t.F) {
+    lo[threadIdx.x] = d_lo ? d_lo[threadIdx.x] : t.lo[threadIdx.x];
+    hi[threadIdx.x] = d_hi ? d_hi[threadIdx.x] : t.hi[threadIdx.x];
+  }
+  if (threadIdx.x == 0) {
+    sh[0] = d_sh ? d_sh[0] : s0;
+    sh[1] = d_sh ? d_sh[1] : s1;
+    sh[2] = d_sh ? d_sh[2] : s2;
+  }
+  __syncthreads();
+}
+
 __global__ void dwt_axis_ref_kernel(const float2* __restrict__ vol, float2* __restrict__ dec, int vx, int vy, int vz,
-                                    int dx, int dy, int dz, int axis, Taps t, int s0, int s1, int s2) {
+                                    int dx, int dy, int dz, int axis, Taps t, int s0, int s1, int s2,
+                                    const float* d_lo, const float* d_hi, const int* d_sh) {
+  __shared__ float lo[20], hi[20];
+  __shared__ int sh[3];
+  load_taps_shift(t, d_lo, d_hi, d_sh, s0, s1, s2, lo, hi, sh);
   const long long tot = (long long)dx * dy * dz;
   const int vs[3] = {vx, vy, vz};
   const int n = vs[axis];
@@ -292,13 +313,12 @@ __global__ void dwt_axis_ref_kernel(const float2* __restrict__ vol, float2* __re
     if (cc >= 2 * nc) continue;
     const bool det = cc >= nc;
     const int k = det ? cc - nc : cc;
-    const float* f = det ? t.hi : t.lo;
+    const float* f = det ? hi : lo;
     float2 acc = make_float2(0.f, 0.f);
     for (int j = 0; j < t.F; ++j) {
       int p[3] = {c[0], c[1], c[2]};
       p[axis] = sym_index(2 * k - t.F + 2 + j, n);
       // circular shift per axis
-      const int sh[3] = {s0, s1, s2};
       for (int a = 0; a < 3; ++a) {
         int v = (p[a] + sh[a]) % vs[a];
         p[a] = v < 0 ? v + vs[a] : v;
@@ -313,7 +333,11 @@ __global__ void dwt_axis_ref_kernel(const float2* __restrict__ vol, float2* __re
 }
 
 __global__ void idwt_axis_ref_kernel(float2* __restrict__ vol, const float2* __restrict__ dec, int vx, int vy, int vz,
-                                     int dx, int dy, int dz, int axis, Taps t, int s0, int s1, int s2) {
+                                     int dx, int dy, int dz, int axis, Taps t, int s0, int s1, int s2,
+                                     const float* d_lo, const float* d_hi, const int* d_sh) {
+  __shared__ float lo[20], hi[20];
+  __shared__ int sh[3];
+  load_taps_shift(t, d_lo, d_hi, d_sh, s0, s1, s2, lo, hi, sh);
   const long long tot = (long long)vx * vy * vz;
   const int ds[3] = {dx, dy, dz};
   const int vs[3] = {vx, vy, vz};
@@ -334,11 +358,10 @@ __global__ void idwt_axis_ref_kernel(float2* __restrict__ vol, const float2* __r
         const float2 av = dec[p[0] + (long long)dx * (p[1] + (long long)dy * p[2])];
         p[axis] = (idx >> 1) + nc;
         const float2 dv = dec[p[0] + (long long)dx * (p[1] + (long long)dy * p[2])];
-        acc.x = fmaf(t.lo[j], av.x, acc.x); acc.y = fmaf(t.lo[j], av.y, acc.y);
-        acc.x = fmaf(t.hi[j], dv.x, acc.x); acc.y = fmaf(t.hi[j], dv.y, acc.y);
+        acc.x = fmaf(lo[j], av.x, acc.x); acc.y = fmaf(lo[j], av.y, acc.y);
+        acc.x = fmaf(hi[j], dv.x, acc.x); acc.y = fmaf(hi[j], dv.y, acc.y);
       }
     }
-    const int sh[3] = {s0, s1, s2};
     int p[3];
     for (int a = 0; a < 3; ++a) {
       int v = (c[a] + sh[a]) % vs[a];
@@ -351,22 +374,26 @@ __global__ void idwt_axis_ref_kernel(float2* __restrict__ vol, const float2* __r
 }  // namespace
 
 int launch_dwt_axis_ref(const float2* vol, float2* dec, const uint32_t* vs, const uint32_t* ds, int axis,
-                        const float* lo, const float* hi, int F, const int* sh, int inverse, cudaStream_t s) {
+                        const float* lo, const float* hi, int F, const int* sh, int inverse, cudaStream_t s,
+                        const float* d_lo, const float* d_hi, const int* d_sh) {
   if (F < 2 || F > 20) return set_error(LLR_ERR_INVALID, "filter length %d outside [2, 20]", F);
   Taps t;
   t.F = F;
-  for (int k = 0; k < F; ++k) { t.lo[k] = lo[k]; t.hi[k] = hi[k]; }
+  for (int k = 0; k < F; ++k) {
+    t.lo[k] = lo ? lo[k] : 0.f;
+    t.hi[k] = hi ? hi[k] : 0.f;
+  }
   const int s0 = sh ? sh[0] : 0, s1 = sh ? sh[1] : 0, s2 = sh ? sh[2] : 0;
   if (!inverse) {
     const long long tot = (long long)ds[0] * ds[1] * ds[2];
     note_launch();
     dwt_axis_ref_kernel<<<grid_for(tot), 256, 0, s>>>(vol, dec, vs[0], vs[1], vs[2], ds[0], ds[1], ds[2], axis, t, s0,
-                                                      s1, s2);
+                                                      s1, s2, d_lo, d_hi, d_sh);
   } else {
     const long long tot = (long long)vs[0] * vs[1] * vs[2];
     note_launch();
     idwt_axis_ref_kernel<<<grid_for(tot), 256, 0, s>>>(const_cast<float2*>(vol), dec, vs[0], vs[1], vs[2], ds[0],
-                                                       ds[1], ds[2], axis, t, s0, s1, s2);
+                                                       ds[1], ds[2], axis, t, s0, s1, s2, d_lo, d_hi, d_sh);
   }
   LLR_CUDA_TRY(cudaGetLastError());
   return LLR_OK;

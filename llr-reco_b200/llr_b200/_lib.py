@@ -129,6 +129,8 @@ SIGNATURES = {
     "llr_cgemm_strided_batched_dev": (C.c_int, [I32, I32, I32, I32, I32, llr_cf32, llr_cf32, I32, I32, P, P, P, P]),
     "llr_dwt3_axis_dev": (C.c_int, [P, P, PU32, PU32, U32, U32, P, P, PI32, P]),
     "llr_idwt3_axis_dev": (C.c_int, [P, P, PU32, PU32, U32, U32, P, P, PI32, P]),
+    "dwt3_axis": (C.c_int, [P, P, PU32, PU32, C.c_uint, C.c_uint, P, P, P]),
+    "idwt3_axis": (C.c_int, [P, P, PU32, PU32, C.c_uint, C.c_uint, P, P, P]),
     "llr_wavelet_denoise_dev": (C.c_int, [P, PI32, I32, I32, I32, F32, P]),
     "llr_hard_project_dev": (C.c_int, [P, P, I64, PF64, P]),
     "llr_cu_low_rank_approx_batch": (C.c_int, [SZ, SZ, SZ, SZ, P]),

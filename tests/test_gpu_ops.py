@@ -296,6 +296,43 @@ def test_dwt_axis_reconstructs_ijk(gpu):
         np.testing.assert_array_equal(np.round(r.real), v.real)
 
 
+def test_reference_dwt_symbols_round_trip_and_shift(gpu):
+    """dwt3_axis / idwt3_axis with the reference's own C signatures (kernels.cu:273,312 as
+    cudwt3.rs:97-100 binds them: host sizes, device filters and device shift pointer):
+    the i+j+k round trip of cudwt3.rs:18-93 on every axis, and a shifted analysis against the
+    oracle with the shift applied per axis."""
+    n = (40, 36, 32)
+    i, j, k = np.meshgrid(*[np.arange(a) for a in n], indexing="ij")
+    v = np.asfortranarray((i + j + k).astype(np.complex64))
+    bank = O.daubechies_bank(2)
+    F = 4
+    filt = [DeviceBuffer.from_array(np.asarray(f, dtype=np.float32)) for f in llr_b200.daubechies_filters(2)]
+    for shift in ((0, 0, 0), (5, -3, 7)):
+        dsh = DeviceBuffer.from_array(np.asarray(shift, dtype=np.int32))
+        vs = np.asarray(n, dtype=np.uint32)
+        for axis in range(3):
+            ds = np.asarray(n, dtype=np.uint32)
+            ds[axis] = 2 * O.sub_band_size(n[axis], F)
+            dv = DeviceBuffer.from_array(v)
+            dd = DeviceBuffer(int(np.prod(ds)) * 8)
+            e = L.lib.dwt3_axis(dv.ptr, dd.ptr, vs.ctypes.data_as(L.PU32), ds.ctypes.data_as(L.PU32), axis, F,
+                                filt[0].ptr, filt[1].ptr, dsh.ptr)
+            assert e == 0
+            dec = dd.download(np.empty(tuple(ds), dtype=np.complex64, order="F"))
+            src = np.roll(v.astype(np.complex128), [-s for s in shift], axis=(0, 1, 2))
+            exp = O.dwt_axis(src, axis, bank.lo_d, bank.hi_d)
+            assert rel_err(dec, exp) < 1e-6, (shift, axis)
+            dv2 = DeviceBuffer(v.nbytes)
+            e = L.lib.idwt3_axis(dv2.ptr, dd.ptr, vs.ctypes.data_as(L.PU32), ds.ctypes.data_as(L.PU32), axis, F,
+                                 filt[2].ptr, filt[3].ptr, dsh.ptr)
+            assert e == 0
+            r = dv2.download(np.empty(n, dtype=np.complex64, order="F"))
+            np.testing.assert_array_equal(np.round(r.real), v.real)
+    bad = np.asarray(n, dtype=np.uint32)
+    assert L.lib.dwt3_axis(dv.ptr, dd.ptr, bad.ctypes.data_as(L.PU32), bad.ctypes.data_as(L.PU32), 0, F,
+                           filt[0].ptr, filt[1].ptr, dsh.ptr) != 0   # decomposition extent too small
+
+
 def test_cu_dwt_denoise_round_trip(gpu):
     """cu_dwt_denoise (cudwt3.rs:102-247): analysis + synthesis without shrink is the identity."""
     rng = np.random.default_rng(17)
