@@ -143,6 +143,10 @@ int llr_ctx_nrmse(llr_ctx* ctx, const llr_cf32* d_ref, double* nrmse);
 /* Number of this library's kernels that one captured iteration launches (cuFFT's kernels
  * are not counted).  Valid after the first llr_iterate* call; no reference counterpart. */
 int llr_ctx_kernel_launches(const llr_ctx* ctx, int32_t* per_iteration);
+/* Blocks the last prox step handed to the Jacobi kernel (more kept components than the
+ * tridiagonal path holds, or eigenvectors failing its residual check); 0 for the Jacobi and
+ * subspace solvers.  Synchronises.  No reference counterpart: a solver diagnostic. */
+int llr_ctx_fallback_blocks(llr_ctx* ctx, int64_t* count);
 int llr_get_iteration(const llr_ctx* ctx, int64_t* it);
 int llr_set_iteration(llr_ctx* ctx, int64_t it);
 /* Residual history of the last `count` iterations ending at the current one. */

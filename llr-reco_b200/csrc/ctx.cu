@@ -788,6 +788,17 @@ int llr_ctx_kernel_launches(const llr_ctx* c, int32_t* per_iteration) {
   return LLR_OK;
 }
 
+int llr_ctx_fallback_blocks(llr_ctx* c, int64_t* count) {
+  if (!c || !count) return set_error(LLR_ERR_INVALID, "null pointer");
+  LLR_CUDA_TRY(cudaSetDevice(c->device));
+  LLR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  int h = 0;
+  if (c->cfg.subspace_rank == 0 && c->cfg.eig_solver != 1)
+    LLR_CUDA_TRY(cudaMemcpy(&h, c->d_fb + std::max<long long>(1, c->nblocks), sizeof(int), cudaMemcpyDeviceToHost));
+  *count = h;
+  return LLR_OK;
+}
+
 int llr_get_iteration(const llr_ctx* c, int64_t* it) {
   if (!c || !it) return set_error(LLR_ERR_INVALID, "null pointer");
   *it = c->h_iter;

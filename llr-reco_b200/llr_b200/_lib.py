@@ -106,6 +106,7 @@ SIGNATURES = {
     "llr_iterate_profiled": (C.c_int, [P, I32, PF64, PF64]),
     "llr_iterate_timed": (C.c_int, [P, I32, PF64]),
     "llr_ctx_kernel_launches": (C.c_int, [P, C.POINTER(I32)]),
+    "llr_ctx_fallback_blocks": (C.c_int, [P, C.POINTER(I64)]),
     "llr_ctx_snapshot": (C.c_int, [P, P]),
     "llr_ctx_nrmse": (C.c_int, [P, P, PF64]),
     "llr_get_iteration": (C.c_int, [P, C.POINTER(I64)]),

@@ -220,6 +220,13 @@ class ReconContext:
         return float(v.value)
 
     @property
+    def fallback_blocks(self) -> int:
+        """Blocks the last prox step handed to the Jacobi kernel."""
+        v = C.c_int64()
+        check(lib.llr_ctx_fallback_blocks(self.h, C.byref(v)))
+        return int(v.value)
+
+    @property
     def kernel_launches_per_iteration(self) -> int:
         """Library kernels (not cuFFT's) one captured iteration launches."""
         v = C.c_int32()

@@ -1,0 +1,79 @@
+"""GPU parity at the benchmark configurations' own sizes (or their shape class where the FP64
+oracle would take minutes), through the C-ABI context against ``oracle.recon``.
+
+Tolerance as in test_gpu_recon.py: relative L2 error of the image <= 2e-4 (complex FP32 vs
+FP64) and of every per-iteration data-consistency residual <= 2e-4.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_err
+from oracle import llr_oracle as O
+
+from llr_b200 import ReconContext, ReconParams, _lib as L
+from llr_b200.phantom import dti_subspace, make_dataset
+
+pytestmark = pytest.mark.gpu
+
+TOL = 2e-4
+
+
+def test_c1_full_configuration(gpu):
+    """Config 1 exactly: 64^3 x 17 (1 b0 + 16 directions at b=1000), 4x VD ky-kz line sampling with
+    a fully sampled 16 x 16 centre, SNR 30, 8^3 blocks (Casorati 512 x 17) with a random shift per
+    iteration, soft threshold 0.02 sigma_max, 50 proximal-gradient iterations (lib.rs:262-341).
+    The blocks the prox hands to the Jacobi kernel are counted every iteration: at most 5 % of
+    the 512 blocks may take that path."""
+    vol, bs, n_iter = (64, 64, 64), (8, 8, 8), 50
+    d = make_dataset(vol, [(0, 1), (1000, 16)], 4.0, 0, centre=16, mask_fn=O.vd_mask)
+    y = d.y
+    ocfg = O.ReconConfig(block_size=bs, mode="soft", seed=11)
+    x0 = O.zero_filled(y.astype(np.complex128), ocfg)
+    ocfg.lam = 0.02 * O.sigma_max(x0, bs)
+    p = ReconParams(vol_size=vol, nq=17, block_size=bs, prox_mode=L.LLR_PROX_SOFT_THRESH, lam=ocfg.lam, seed=11)
+    hist, fallback = [], []
+    with ReconContext(p) as ctx:
+        ctx.upload_kspace(y)
+        ctx.init_zero_filled()
+        assert rel_err(ctx.download_image(), x0) < 2e-6
+        for _ in range(n_iter):
+            hist.extend(ctx.iterate(1))
+            fallback.append(ctx.fallback_blocks)
+        gx = ctx.download_image()
+    ox, oh = O.recon(y.astype(np.complex128), ocfg, n_iter, x0=x0)
+    print(f"C1: image rel err {rel_err(gx, ox):.2e}; Jacobi-fallback blocks per iteration: max {max(fallback)}, "
+          f"mean {np.mean(fallback):.2f} of 512")
+    assert np.all(np.isfinite(hist))
+    assert rel_err(gx, ox) < TOL, rel_err(gx, ox)
+    np.testing.assert_allclose(hist, oh, rtol=TOL)
+    assert max(fallback) <= 0.05 * 512, fallback
+
+
+def test_c3_shape_class(gpu):
+    """Config-3 shape class: 61 volumes (b = 0 / 1000 / 2000, 1 / 30 / 30), 10x sampling, rank-7
+    temporal subspace, LLR on the subspace coefficients with 8^3 blocks (X <- LR(X S) S^H,
+    dti_subspace.rs:141-221), soft threshold 0.02 sigma_max, then the 3-level db4 wavelet shrink with
+    alpha 0.005 on every volume (lib.rs:430-465); a 64 x 56 x 56 volume, the smallest on which a
+    3-level db4 decomposition runs along every axis."""
+    vol, bs, n_iter = (64, 56, 56), (8, 8, 8), 2
+    d = make_dataset(vol, [(0, 1), (1000, 30), (2000, 30)], 10.0, 0, centre=16, mask_fn=O.vd_mask)
+    S = dti_subspace(d.b, d.g, 7, 20000, 1)
+    y = d.y
+    ocfg = O.ReconConfig(block_size=bs, mode="soft", seed=13, wavelet_alpha=0.005, wavelet_moments=4,
+                         wavelet_levels=3)
+    ocfg.subspace = S.astype(np.complex128)
+    x0 = O.zero_filled(y.astype(np.complex128), ocfg)
+    ocfg.lam = 0.02 * O.sigma_max(x0, bs)
+    p = ReconParams(vol_size=vol, nq=61, block_size=bs, prox_mode=L.LLR_PROX_SOFT_THRESH, lam=ocfg.lam, seed=13,
+                    subspace_rank=7)
+    p.wavelet_alpha, p.wavelet_moments, p.wavelet_levels = 0.005, 4, 3
+    with ReconContext(p) as ctx:
+        ctx.upload_kspace(y)
+        ctx.upload_subspace(S)
+        ctx.init_zero_filled()
+        hist = ctx.iterate(n_iter)
+        gx = ctx.download_image()
+    ox, oh = O.recon(y.astype(np.complex128), ocfg, n_iter, x0=x0)
+    assert np.all(np.isfinite(hist))
+    assert rel_err(gx, ox) < TOL, rel_err(gx, ox)
+    np.testing.assert_allclose(hist, oh, rtol=TOL)
