@@ -273,8 +273,10 @@ def workload_label(name: str, c: dict, nq: int) -> str:
     n = c.get("srank", nq)
     extra = ""
     if "srank" in c:
+        where = "subspace coefficient volumes" if c.get("wavelet_space", 0) else "image volumes"
         extra = (f", rank-{c['srank']} temporal subspace (LLR on coefficients), "
-                 f"{c['wavelet_levels']}-level db{c['wavelet_moments']} wavelet shrink alpha {c['wavelet_alpha']:g}")
+                 f"{c['wavelet_levels']}-level db{c['wavelet_moments']} wavelet shrink alpha {c['wavelet_alpha']:g} "
+                 f"on the {where}")
     return (f"{name}: {v[0]}x{v[1]}x{v[2]} complex64 x {nq} volumes, {b[0]}^3 LLR blocks (Casorati "
             f"{b[0] * b[1] * b[2]}x{n}){extra}, {c['accel']:g}x VD line sampling, soft threshold 0.02 sigma_max, "
             f"FP32, one proximal-gradient iteration per step")
@@ -301,6 +303,7 @@ def run_b200(args, dist: Dist) -> None:
         params.subspace_rank = c["srank"]
         params.wavelet_alpha, params.wavelet_moments = c["wavelet_alpha"], c["wavelet_moments"]
         params.wavelet_levels = c["wavelet_levels"]
+        params.wavelet_space = c.get("wavelet_space", 0)
     ctx = ReconContext(params)
     if "srank" in c:
         ctx.upload_subspace(dti_subspace_gpu(d.b, d.g, c["srank"], 100000, args.seed)[0])

@@ -71,7 +71,14 @@ typedef struct llr_config {
   int32_t gram_mode;          /* 0: 3xTF32 tensor cores (default); 1: FP32 FMA        */
   int32_t fft_mode;           /* 0: fused FFT + DC + inverse FFT per (x, volume) plane
                                   where the plane fits (default); 1: cuFFT passes       */
-  int32_t reserved[4];
+  int32_t wavelet_space;      /* with a subspace: 0 = shrink the wavelet coefficients of
+                                  every image volume (lib.rs:302-309, the reference);
+                                  1 = of the srank subspace coefficient volumes (the
+                                  blocks must tile the volume)                           */
+  int32_t block_stride[3];    /* 0 -> block size (non-overlapping grid, block.rs:112-133);
+                                  s < b: overlapping blocks every s voxels, each voxel
+                                  the mean of its (b/s)^3 block outputs (b % s == 0 and
+                                  the blocks must tile the volume)                       */
 } llr_config;
 
 /* ---- library / errors ------------------------------------------------------------ */

@@ -184,6 +184,13 @@ static bool defer_zero_blocks(const llr_ctx* c) {
          (long long)c->gy * c->gz <= 4096;
 }
 
+// Inside an iteration with a subspace and wavelet_space == 1, the prox stores the subspace
+// coefficient volumes LR(X S) in d_work, the wavelet shrinks those srank volumes, and an expand
+// kernel writes X = C S^H (the FFT input) back to d_x.
+static bool coef_mode(const llr_ctx* c) {
+  return c->cfg.subspace_rank > 0 && c->wavelet_on && c->cfg.wavelet_space == 1;
+}
+
 // One prox pass on d_x.  standalone == true keeps the raw convention (used by single-step
 // entry points); otherwise the output is the FFT input (or the image, if the wavelet runs).
 static int prox_pass(llr_ctx* c, cudaStream_t s, const int* explicit_shift, bool standalone, float* block_stat) {
@@ -200,6 +207,10 @@ static int prox_pass(llr_ctx* c, cudaStream_t s, const int* explicit_shift, bool
     op.m = c->m; op.nq = c->g.nq; op.srank = c->cfg.subspace_rank;
     op.mode = c->cfg.prox_mode; op.rank = c->cfg.rank; op.lambda = c->cfg.lambda;
     op.S = c->d_S;
+    if (!standalone && coef_mode(c)) {
+      op.coef_out = c->d_work;
+      return launch_llr_prox_subspace(src, op, s);   // the blocks tile the volume (validated)
+    }
     LLR_TRY(launch_llr_prox_subspace(src, op, s));
   } else {
     ProxOp op;
@@ -226,9 +237,22 @@ static int prox_pass(llr_ctx* c, cudaStream_t s, const int* explicit_shift, bool
   return LLR_OK;
 }
 
-// Wavelet shrink on the image held in d_x; stores e^{+i theta_ksp} x * store_scale.
-static int wavelet_pass(llr_ctx* c, cudaStream_t s, float store_scale) {
+// Wavelet shrink on the image held in d_x; stores e^{+i theta_ksp} x * store_scale.  In an
+// iteration in coefficient mode: shrink the coefficient volumes in d_work, then expand them into
+// d_x as the FFT input.
+static int wavelet_pass(llr_ctx* c, cudaStream_t s, float store_scale, bool in_iteration = false) {
   const long long sx = c->g.nyz, sy = 1, sz = c->g.ny, sv = c->g.V;
+  if (in_iteration && coef_mode(c)) {
+    const int sr = c->cfg.subspace_rank;
+    const int nb = std::max(1, (int)(c->wavelet_work_elems / wavelet_workspace_elems(c->wplan, 1)));
+    PhaseTab none{nullptr, nullptr, nullptr};
+    for (int k0 = 0; k0 < sr; k0 += nb)
+      LLR_TRY(wavelet_denoise_strided_xf(c->wplan, c->d_work + (size_t)k0 * c->g.V, sx, sy, sz, sv,
+                                         std::min(nb, sr - k0), c->cfg.wavelet_alpha, c->d_wavelet_work, none,
+                                         nullptr, 0, 1.f, s));
+    return launch_subspace_expand(c->d_work, c->d_x, c->d_S, sr, c->g, ctx_phase(c, c->d_ph_ksp, !c->hybrid), 1,
+                                  store_scale, s);
+  }
   const int nb = std::max(1, (int)(c->wavelet_work_elems / wavelet_workspace_elems(c->wplan, 1)));
   PhaseTab ph = ctx_phase(c, c->d_ph_ksp, !c->hybrid);
   for (int q0 = 0; q0 < c->g.nq; q0 += nb) {
@@ -261,7 +285,7 @@ static int fused_dc_pass(llr_ctx* c, cudaStream_t s, double* out) {
 
 int ctx_enqueue_iteration(llr_ctx* c, cudaStream_t s) {
   LLR_TRY(prox_pass(c, s, nullptr, false, nullptr));
-  if (c->wavelet_on) LLR_TRY(wavelet_pass(c, s, 1.f));
+  if (c->wavelet_on) LLR_TRY(wavelet_pass(c, s, 1.f, true));
   if (c->fused_fft) return fused_dc_pass(c, s, nullptr);
   LLR_TRY(exec_fft(c, c->d_x, CUFFT_FORWARD, s));
   LLR_TRY(dc_pass(c, s, 0));
@@ -614,7 +638,7 @@ static int capture_stage(llr_ctx* c, int stage, cudaGraphExec_t* out) {
   int st = LLR_OK;
   switch (stage) {
     case 0: st = prox_pass(c, s, nullptr, false, nullptr); break;
-    case 1: if (c->wavelet_on) st = wavelet_pass(c, s, 1.f); break;
+    case 1: if (c->wavelet_on) st = wavelet_pass(c, s, 1.f, true); break;
     case 2: st = c->fused_fft ? fused_dc_pass(c, s, nullptr) : exec_fft(c, c->d_x, CUFFT_FORWARD, s); break;
     case 3:
       if (c->fused_fft) break;

@@ -194,6 +194,22 @@ int llr_config_validate(const llr_config* c) {
   if (c->fft_mode != 0 && c->fft_mode != 1) return set_error(LLR_ERR_INVALID, "fft_mode must be 0 or 1");
   if (c->wavelet_alpha > 0.f && (c->wavelet_moments < 1 || c->wavelet_moments > 10))
     return set_error(LLR_ERR_INVALID, "wavelet_moments must be in [1, 10]");
+  if (c->wavelet_space != 0 && c->wavelet_space != 1) return set_error(LLR_ERR_INVALID, "wavelet_space must be 0 or 1");
+  bool tiles = true, overlap = false;
+  for (int a = 0; a < 3; ++a) {
+    const int b = c->block_size[a], st = c->block_stride[a];
+    if (st < 0 || st > b) return set_error(LLR_ERR_INVALID, "block_stride[%d] must be in [0, block size]", a);
+    if (st > 0 && st < b) {
+      overlap = true;
+      if (b % st != 0) return set_error(LLR_ERR_INVALID, "block size must be a multiple of block_stride");
+    }
+    if (c->vol_size[a] % b != 0) tiles = false;
+  }
+  if (overlap && !tiles) return set_error(LLR_ERR_UNSUPPORTED, "overlapping blocks need a volume the blocks tile");
+  if (overlap && c->subspace_rank > 0)
+    return set_error(LLR_ERR_UNSUPPORTED, "overlapping blocks are not combined with a subspace");
+  if (c->wavelet_space == 1 && c->subspace_rank > 0 && c->wavelet_alpha > 0.f && !tiles)
+    return set_error(LLR_ERR_UNSUPPORTED, "subspace-coefficient wavelet needs a volume the blocks tile");
   if (m < 1) return set_error(LLR_ERR_INVALID, "empty block");
   const long long E = (long long)c->vol_size[0] * c->vol_size[1] * c->vol_size[2] * c->nq;
   if (E >= (1LL << 31) * 2) return set_error(LLR_ERR_UNSUPPORTED, "dataset of %lld elements too large", E);

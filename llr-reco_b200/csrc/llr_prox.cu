@@ -233,6 +233,90 @@ __global__ void __launch_bounds__(kLlrThreads) llr_subspace_kernel(BlockSource s
   }
 }
 
+// Coefficient output: the same gather and low-rank step, storing Z' = LR(X S) as srank
+// planar coefficient volumes (image space) for a shrink in the coefficient domain.
+template <int NPMAX>
+__global__ void __launch_bounds__(kLlrThreads) llr_subspace_coef_kernel(BlockSource src, SubspaceOp op, SmemLayout L) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  Misc* misc = reinterpret_cast<Misc*>(smem);
+  float4* rot = reinterpret_cast<float4*>(smem + L.off_rot);
+  int2* pairs = reinterpret_cast<int2*>(smem + L.off_pair);
+  float* ev = reinterpret_cast<float*>(smem + L.off_ev);
+  float* g = reinterpret_cast<float*>(smem + L.off_g);
+  int* act = reinterpret_cast<int*>(smem + L.off_act);
+  float2* A = reinterpret_cast<float2*>(smem + L.off_A);
+  float2* V = reinterpret_cast<float2*>(smem + L.off_V);
+  float2* scr = reinterpret_cast<float2*>(smem + L.off_scr);
+  float2* Z = reinterpret_cast<float2*>(smem + L.off_C);
+  float2* Ss = Z + (size_t)op.srank * L.ldc;
+  const int m = op.m, nq = op.nq, sr = op.srank;
+  for (int i = threadIdx.x; i < nq * sr; i += blockDim.x) {
+    const int q = i / sr, k = i - q * sr;
+    Ss[i] = op.S[q + (long long)nq * k];
+  }
+  if (threadIdx.x == 0) block_shift(src, misc->shift);
+  __syncthreads();
+  int sh[3] = {misc->shift[0], misc->shift[1], misc->shift[2]};
+  Geom gc = src.g;
+  gc.nq = sr;
+  for (long long blk = blockIdx.x; blk < src.nblocks; blk += gridDim.x) {
+    for (int r = threadIdx.x; r < m; r += blockDim.x) {
+      float2 z[kSubMax];
+#pragma unroll
+      for (int k = 0; k < kSubMax; ++k) z[k] = make_float2(0.f, 0.f);
+      int ix = 0, iy = 0, iz = 0;
+      block_row_coord(src, blk, sh, r, ix, iy, iz);
+      for (int q = 0; q < nq; ++q) {
+        float2 v = src.data[planar_index(src.g, ix, iy, iz, q)];
+        v = cscale(cmul_bc(v, phase_at(src.ph, src.g, q, ix, iy, iz)), src.load_scale);
+#pragma unroll
+        for (int k = 0; k < kSubMax; ++k)
+          if (k < sr) cfma(z[k], v, Ss[q * sr + k]);
+      }
+#pragma unroll
+      for (int k = 0; k < kSubMax; ++k)
+        if (k < sr) Z[k * L.ldc + r] = z[k];
+    }
+    __syncthreads();
+    gram<NPMAX, 2>(Z, L.ldc, m, sr, A, scr, L.ksplit);
+    jacobi<NPMAX>(A, V, sr, rot, pairs, misc, 16);
+    singular_map(A, NPMAX + 1, sr, op.mode, op.rank, op.lambda, ev, g, act, misc);
+    form_W(A, V, NPMAX + 1, sr, g, act, misc->n_active);
+    apply_W<NPMAX, 2>(Z, L.ldc, m, sr, A);
+    for (int r = threadIdx.x; r < m; r += blockDim.x) {
+      int ix = 0, iy = 0, iz = 0;
+      block_row_coord(src, blk, sh, r, ix, iy, iz);
+      for (int k = 0; k < sr; ++k) op.coef_out[planar_index(gc, ix, iy, iz, k)] = Z[k * L.ldc + r];
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(256) subspace_expand_kernel(const float2* __restrict__ coef, float2* __restrict__ x,
+                                                              const float2* __restrict__ S, int srank, Geom g,
+                                                              PhaseTab ph, int store_phase, float scale) {
+  __shared__ float2 Ss[64 * kSubMax];
+  for (int i = threadIdx.x; i < g.nq * srank; i += blockDim.x) Ss[i] = S[i];   // column-major (q, k)
+  __syncthreads();
+  for (long long v = blockIdx.x * 256LL + threadIdx.x; v < g.V; v += (long long)gridDim.x * 256) {
+    float2 c[kSubMax];
+#pragma unroll
+    for (int k = 0; k < kSubMax; ++k) c[k] = k < srank ? coef[v + g.V * k] : make_float2(0.f, 0.f);
+    const int iy = (int)(v % g.ny);
+    const long long r = v / g.ny;
+    const int iz = (int)(r % g.nz), ix = (int)(r / g.nz);
+    for (int q = 0; q < g.nq; ++q) {
+      float2 a = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int k = 0; k < kSubMax; ++k)
+        if (k < srank) cfma_cb(a, c[k], Ss[q + g.nq * k]);
+      a = cscale(a, scale);
+      if (store_phase) a = cmul(a, phase_at(ph, g, q, ix, iy, iz));
+      x[v + g.V * q] = a;
+    }
+  }
+}
+
 }  // namespace
 
 int launch_llr_prox_subspace(const BlockSource& src, const SubspaceOp& op, cudaStream_t stream) {
@@ -242,7 +326,8 @@ int launch_llr_prox_subspace(const BlockSource& src, const SubspaceOp& op, cudaS
   SmemLayout L = make_layout<16, 2>(op.m, op.srank);
   L.total = align16(L.total + sizeof(float2) * (size_t)op.nq * op.srank);
   if (L.total > 227 * 1024) return set_error(LLR_ERR_UNSUPPORTED, "subspace prox needs %zu B smem", L.total);
-  auto kern = llr_subspace_kernel<16>;
+  if (op.coef_out && src.kind != 1) return set_error(LLR_ERR_INVALID, "coefficient output needs volume blocks");
+  auto kern = op.coef_out ? llr_subspace_coef_kernel<16> : llr_subspace_kernel<16>;
   LLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total));
     LLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   int dev = 0, nsm = 0, occ = 0;
@@ -309,6 +394,16 @@ int launch_lift(const float2* vol, float2* mat, const int* vs, int nq, const int
 // =======================================================================================
 // rhsCdgmmBatched (kernels.cu:11-67) and a batched complex GEMM with the semantics of
 // cublas_cgemm_strided_batched_device (cublas.rs:12-105).
+int launch_subspace_expand(const float2* coef, float2* x, const float2* S, int srank, const Geom& g, PhaseTab ph,
+                           int store_phase, float scale, cudaStream_t s) {
+  if (srank < 1 || srank > kSubMax || g.nq > 64) return set_error(LLR_ERR_UNSUPPORTED, "subspace expand shape");
+  const long long blocks = std::min<long long>((g.V + 255) / 256, 148LL * 16);
+  note_launch();
+  subspace_expand_kernel<<<(unsigned)blocks, 256, 0, s>>>(coef, x, S, srank, g, ph, store_phase, scale);
+  LLR_CUDA_TRY(cudaGetLastError());
+  return LLR_OK;
+}
+
 // =======================================================================================
 namespace {
 

@@ -56,7 +56,8 @@ class llr_config(C.Structure):
         ("eig_solver", C.c_int32),
         ("gram_mode", C.c_int32),
         ("fft_mode", C.c_int32),
-        ("reserved", C.c_int32 * 4),
+        ("wavelet_space", C.c_int32),
+        ("block_stride", C.c_int32 * 3),
     ]
 
 

@@ -117,6 +117,8 @@ class ReconParams:
     eig_solver: int = 0
     gram_mode: int = 0
     fft_mode: int = 0
+    wavelet_space: int = 0
+    block_stride: Optional[Sequence[int]] = None
 
     def to_c(self) -> L.llr_config:
         c = L.llr_config()
@@ -138,6 +140,8 @@ class ReconParams:
         c.eig_solver = int(self.eig_solver)
         c.gram_mode = int(self.gram_mode)
         c.fft_mode = int(self.fft_mode)
+        c.wavelet_space = int(self.wavelet_space)
+        c.block_stride = L.i32x3(self.block_stride or (0, 0, 0))
         return c
 
 

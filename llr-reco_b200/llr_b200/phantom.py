@@ -163,7 +163,7 @@ CONFIGS = {
     # config-2 geometry class at 1/8 of the volume (216 MB per copy, still > L2): profiling case
     "c2_small": dict(vol=(96, 96, 48), shells=[(0, 7), (3000, 54)], accel=8.0, block=(6, 6, 6), n_iter=100),
     "c3": dict(vol=(256, 256, 256), shells=[(0, 1), (1000, 30), (2000, 30)], accel=10.0, block=(8, 8, 8),
-               n_iter=80, srank=7, wavelet_alpha=0.005, wavelet_moments=4, wavelet_levels=3),
+               n_iter=80, srank=7, wavelet_alpha=0.005, wavelet_moments=4, wavelet_levels=3, wavelet_space=1),
 }
 
 

@@ -618,6 +618,21 @@ class ReconConfig:
     subspace: Optional[np.ndarray] = None
     lin_ksp: Optional[np.ndarray] = None
     lin_img: Optional[np.ndarray] = None
+    wavelet_space: str = "image"  # with a subspace: "image" (lib.rs:302-309) | "coeffs" (srank volumes)
+
+
+def llr_prox_coeffs(x: np.ndarray, cfg: ReconConfig, shift) -> np.ndarray:
+    """The subspace prox of lib.rs:281-289 stopped before the back-projection: the coefficient
+    volumes LR(X S) (nx, ny, nz, srank), blocks un-lifted into them (the blocks tile the volume)."""
+    nx, ny, nz, nq = x.shape
+    S = np.asarray(cfg.subspace)
+    nb = int(np.prod(grid_dim((nx, ny, nz), cfg.block_size)))
+    mats = lift_data_set(np.asfortranarray(x), cfg.block_size, shift, 0, nb)
+    Z = np.einsum("mqb,qk->mkb", mats, S)
+    Z = low_rank_hard(Z, cfg.rank) if cfg.mode == "hard" else low_rank_soft(Z, cfg.lam)
+    out = np.zeros((nx, ny, nz, S.shape[1]), dtype=np.result_type(x.dtype, S.dtype), order="F")
+    un_lift_data_set(out, Z, cfg.block_size, shift, 0, nb)
+    return out
 
 
 def llr_prox(x: np.ndarray, cfg: ReconConfig, shift) -> np.ndarray:
@@ -654,8 +669,17 @@ def iterate(x: np.ndarray, y: np.ndarray, cfg: ReconConfig, it: int):
     nx, ny, nz, nq = x.shape
     maxs = cfg.max_rand_shift or (nx, ny, nz)
     shift = rand_shift(cfg.seed, it, maxs)
-    z = llr_prox(x, cfg, shift)
-    if cfg.wavelet_alpha > 0:
+    coeffs = cfg.subspace is not None and cfg.wavelet_alpha > 0 and cfg.wavelet_space == "coeffs"
+    if coeffs:
+        # shrink in the subspace coefficient domain, then X = C S^H
+        c = llr_prox_coeffs(x, cfg, shift)
+        bank = daubechies_bank(cfg.wavelet_moments)
+        for k in range(c.shape[3]):
+            c[..., k] = wavelet_denoise(c[..., k], cfg.wavelet_alpha, bank, cfg.wavelet_levels)
+        z = np.asfortranarray(np.einsum("xyzk,qk->xyzq", c, np.conj(cfg.subspace)))
+    else:
+        z = llr_prox(x, cfg, shift)
+    if cfg.wavelet_alpha > 0 and not coeffs:
         bank = daubechies_bank(cfg.wavelet_moments)
         for q in range(nq):
             z[..., q] = wavelet_denoise(z[..., q], cfg.wavelet_alpha, bank, cfg.wavelet_levels)

@@ -77,3 +77,31 @@ def test_c3_shape_class(gpu):
     assert np.all(np.isfinite(hist))
     assert rel_err(gx, ox) < TOL, rel_err(gx, ox)
     np.testing.assert_allclose(hist, oh, rtol=TOL)
+
+
+def test_c3_coefficient_wavelet(gpu):
+    """Config 3 as run by the benchmark: the 3-level db4 shrink (alpha 0.005) acts on the 7 subspace
+    coefficient volumes LR(X S) and the image is C S^H (wavelet_space 1); 64^3 x 61, 10x sampling,
+    8^3 blocks, soft threshold 0.02 sigma_max, 3 iterations against the oracle's coefficient form."""
+    vol, bs, n_iter = (64, 64, 64), (8, 8, 8), 3
+    d = make_dataset(vol, [(0, 1), (1000, 30), (2000, 30)], 10.0, 1, centre=16, mask_fn=O.vd_mask)
+    S = dti_subspace(d.b, d.g, 7, 20000, 2)
+    y = d.y
+    ocfg = O.ReconConfig(block_size=bs, mode="soft", seed=17, wavelet_alpha=0.005, wavelet_moments=4,
+                         wavelet_levels=3, wavelet_space="coeffs")
+    ocfg.subspace = S.astype(np.complex128)
+    x0 = O.zero_filled(y.astype(np.complex128), ocfg)
+    ocfg.lam = 0.02 * O.sigma_max(x0, bs)
+    p = ReconParams(vol_size=vol, nq=61, block_size=bs, prox_mode=L.LLR_PROX_SOFT_THRESH, lam=ocfg.lam, seed=17,
+                    subspace_rank=7, wavelet_space=1)
+    p.wavelet_alpha, p.wavelet_moments, p.wavelet_levels = 0.005, 4, 3
+    with ReconContext(p) as ctx:
+        ctx.upload_kspace(y)
+        ctx.upload_subspace(S)
+        ctx.init_zero_filled()
+        hist = ctx.iterate(n_iter)
+        gx = ctx.download_image()
+    ox, oh = O.recon(y.astype(np.complex128), ocfg, n_iter, x0=x0)
+    assert np.all(np.isfinite(hist))
+    assert rel_err(gx, ox) < TOL, rel_err(gx, ox)
+    np.testing.assert_allclose(hist, oh, rtol=TOL)

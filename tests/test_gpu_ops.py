@@ -344,7 +344,8 @@ def test_cu_dwt_denoise_round_trip(gpu):
     assert rel_err(buf, x.reshape(-1, order="F")) < 2e-6
 
 
-@pytest.mark.parametrize("vol,moments,levels", [((32, 32, 32), 2, 0), ((40, 36, 28), 4, 2), ((33, 30, 26), 2, 2)])
+@pytest.mark.parametrize("vol,moments,levels", [((32, 32, 32), 2, 0), ((40, 36, 28), 4, 2), ((33, 30, 26), 2, 2),
+                                                 ((70, 50, 45), 4, 3), ((24, 20, 18), 1, 2), ((40, 40, 40), 8, 1)])
 def test_wavelet_denoise_matches_oracle(gpu, vol, moments, levels):
     rng = np.random.default_rng(18)
     nvol = 2
