@@ -183,7 +183,8 @@ int llr_lift_data_set_dev(const llr_cf32* d_vol, int32_t nq, llr_cf32* d_mat,
 int llr_un_lift_data_set_dev(llr_cf32* d_vol, int32_t nq, const llr_cf32* d_mat,
                              const int32_t vol_size[3], const int32_t block_size[3],
                              const int32_t shift[3], int64_t start, int64_t n, void* stream);
-/* cu_low_rank_approx_batch (low_rank.rs:10-69) in place on (m, n, batch), n <= 64. */
+/* cu_low_rank_approx_batch (low_rank.rs:10-69) in place on (m, n, batch), n <= 128 (n > 64 runs
+ * the wide Jacobi kernel). */
 int llr_low_rank_batch_dev(int32_t m, int32_t n, int32_t rank, int32_t batch,
                            llr_cf32* d_mats, void* stream);
 /* Same operation as llr_low_rank_batch_dev, for callers that cannot let the library
@@ -202,7 +203,7 @@ int llr_low_rank_batch_dev(int32_t m, int32_t n, int32_t rank, int32_t batch,
  * streams, race: serialise them. */
 int llr_low_rank_batch_dev_noalloc(int32_t m, int32_t n, int32_t rank, int32_t batch,
                                    llr_cf32* d_mats, void* stream);
-/* Singular-value soft threshold of every (m, n) matrix, n <= 64. */
+/* Singular-value soft threshold of every (m, n) matrix, n <= 128. */
 int llr_soft_threshold_batch_dev(int32_t m, int32_t n, float lambda, int32_t batch,
                                  llr_cf32* d_mats, void* stream);
 /* LR(X S) S^H per Casorati matrix (lib.rs:281-289, dti_subspace.rs:141-221). */

@@ -179,7 +179,7 @@ static BlockSource make_source(llr_ctx* c, const int* explicit_shift, float stor
 // path (warp eigen kernel + apply kernel) reports such blocks, and nothing may read the iterate
 // between the two stages (no wavelet stage).
 static bool defer_zero_blocks(const llr_ctx* c) {
-  return c->fused_fft && !c->wavelet_on && c->cfg.subspace_rank == 0 && c->cfg.eig_solver == 0 &&
+  return c->fused_fft && !c->wavelet_on && c->phase_off.empty() && c->cfg.subspace_rank == 0 && c->cfg.eig_solver == 0 &&
          c->d_gram != nullptr && c->d_blk_ra != nullptr && c->g.nq <= 64 &&
          (long long)c->gy * c->gz <= 4096;
 }
@@ -225,6 +225,24 @@ static int prox_pass(llr_ctx* c, cudaStream_t s, const int* explicit_shift, bool
     op.gram_mode = c->cfg.gram_mode;
     op.err = c->d_err;
     op.defer_zero = (!standalone && !block_stat && !explicit_shift && defer_zero_blocks(c)) ? 1 : 0;
+    op.vwide = c->d_vwide;
+    op.vwide_ctas = c->vwide_ctas;
+    if (!c->phase_off.empty() && !block_stat) {
+      // overlapping blocks: every phase of the strided grid is a non-overlapping tiling at the
+      // shift plus the phase offset; the mean of the phases goes to d_work, then back to d_x
+      const int P = (int)c->phase_off.size() / 3;
+      for (int p = 0; p < P; ++p) {
+        BlockSource ps = src;
+        ps.ox = c->phase_off[3 * p]; ps.oy = c->phase_off[3 * p + 1]; ps.oz = c->phase_off[3 * p + 2];
+        ps.out = c->d_work;
+        ps.accumulate = p > 0;
+        ps.store_scale = src.store_scale / (float)P;
+        LLR_TRY(launch_llr_prox(ps, op, s));
+      }
+      LLR_CUDA_TRY(cudaMemcpyAsync(c->d_x, c->d_work, sizeof(float2) * (size_t)c->g.V * c->g.nq,
+                                   cudaMemcpyDeviceToDevice, s));
+      return LLR_OK;   // the blocks tile the volume (validated)
+    }
     LLR_TRY(launch_llr_prox(src, op, s));
   }
   if (block_stat || standalone) return LLR_OK;
@@ -347,9 +365,29 @@ int llr_ctx_create(const llr_config* cfg, llr_ctx** out) {
   if ((st = dalloc(&c->d_block_stat, (size_t)std::max<long long>(1, c->nblocks)))) return fail(st);
   if ((st = dalloc(&c->d_fb, (size_t)std::max<long long>(1, c->nblocks) + 1))) return fail(st);
   if ((st = dalloc(&c->d_err, 1))) return fail(st);
+  if (cfg->subspace_rank == 0 && c->g.nq > 64) {
+    c->vwide_ctas = wide_jacobi_ctas();
+    if ((st = dalloc(&c->d_vwide, (size_t)c->vwide_ctas * (size_t)wide_v_stride()))) return fail(st);
+  }
+  {
+    int per[3], P = 1;
+    for (int a = 0; a < 3; ++a) {
+      const int b = cfg->block_size[a], st2 = cfg->block_stride[a];
+      per[a] = (st2 > 0 && st2 < b) ? b / st2 : 1;
+      P *= per[a];
+    }
+    if (P > 1)
+      for (int pz = 0; pz < per[2]; ++pz)
+        for (int py = 0; py < per[1]; ++py)
+          for (int px = 0; px < per[0]; ++px) {
+            c->phase_off.push_back(px * (per[0] > 1 ? cfg->block_stride[0] : 0));
+            c->phase_off.push_back(py * (per[1] > 1 ? cfg->block_stride[1] : 0));
+            c->phase_off.push_back(pz * (per[2] > 1 ? cfg->block_stride[2] : 0));
+          }
+  }
   e = cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream);
   if (e != cudaSuccess) return fail(cuda_error(e, "cudaMemsetAsync", __FILE__, __LINE__));
-  if (cfg->subspace_rank == 0 &&
+  if (cfg->subspace_rank == 0 && c->g.nq <= 64 &&
       ((st = dalloc(&c->d_gram, (size_t)std::max<long long>(1, c->nblocks) * (size_t)prox_gram_stride(c->g.nq))) ||
        (st = dalloc(&c->d_blk_ra, (size_t)std::max<long long>(1, c->nblocks) + 1))))
     return fail(st);
@@ -395,7 +433,7 @@ int llr_ctx_destroy(llr_ctx* c) {
   if (c->have_plan) cufftDestroy(c->plan_fwd);
   dfree(c->d_x); dfree(c->d_work); dfree(c->d_yhat); dfree(c->d_samp_pos); dfree(c->d_samp_off);
   dfree(c->d_ph_ksp); dfree(c->d_ph_img); dfree(c->d_S); dfree(c->d_partials); dfree(c->d_hist); dfree(c->d_iter);
-  dfree(c->d_block_stat); dfree(c->d_fb); dfree(c->d_gram); dfree(c->d_blk_ra); dfree(c->d_fft_tw); dfree(c->d_err); dfree(c->d_wavelet_work); dfree(c->d_fft_work);
+  dfree(c->d_block_stat); dfree(c->d_fb); dfree(c->d_gram); dfree(c->d_blk_ra); dfree(c->d_fft_tw); dfree(c->d_err); dfree(c->d_vwide); dfree(c->d_wavelet_work); dfree(c->d_fft_work);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return LLR_OK;
@@ -936,6 +974,7 @@ int llr_ctx_device_bytes(const llr_ctx* c, size_t* bytes) {
   b += c->hybrid ? (size_t)c->n_samp_lines * c->g.nx * sizeof(float2) : (c->have_kspace ? E * sizeof(float2) : 0);
   b += c->fft_work_bytes + c->wavelet_work_elems * sizeof(float2);
   if (c->d_gram) b += (size_t)std::max<long long>(1, c->nblocks) * (size_t)prox_gram_stride(c->g.nq) * sizeof(float2);
+  if (c->d_vwide) b += (size_t)c->vwide_ctas * (size_t)wide_v_stride() * sizeof(float2);
   *bytes = b;
   return LLR_OK;
 }

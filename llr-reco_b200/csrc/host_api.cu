@@ -390,7 +390,19 @@ static int batch_prox(int m, int n, int mode, int rank, float lam, int batch, ll
   op.gram_stride = prox_gram_stride(n);
   op.gram_mode = 0;
   op.err = nullptr;
+  float2* vwide = nullptr;
+  if (n > 64 && n <= kProxMaxN) {   // eigenvector scratch of the wide Jacobi kernel
+    op.vwide_ctas = wide_jacobi_ctas();
+    e = cudaMallocAsync((void**)&vwide, sizeof(float2) * (size_t)op.vwide_ctas * (size_t)wide_v_stride(), s);
+    if (e != cudaSuccess) {
+      cudaFreeAsync(fb, s);
+      cudaFreeAsync(gram, s);
+      return cuda_error(e, "cudaMallocAsync", __FILE__, __LINE__);
+    }
+    op.vwide = vwide;
+  }
   int st = launch_llr_prox(src, op, s);
+  if (vwide) cudaFreeAsync(vwide, s);
   e = cudaFreeAsync(fb, s);
   cudaError_t e2 = cudaFreeAsync(gram, s);
   if (st == LLR_OK && e != cudaSuccess) st = cuda_error(e, "cudaFreeAsync", __FILE__, __LINE__);

@@ -31,6 +31,9 @@ struct BlockSource {
   int ph_uniform;      // every volume has the same phase tables (per-row phase suffices)
   const int* blk_list; // optional list of block indices (with blk_count) instead of 0..nblocks-1
   const int* blk_count;
+  int ox, oy, oz;      // offset added to the (drawn or explicit) shift: one phase of an overlapping grid
+  float2* out;         // null: results go back to `data`; else to `out` (same layout; planar only)
+  int accumulate;      // with `out`: out += result (zero results are skipped) instead of out = result
 };
 
 struct ProxOp {
@@ -49,7 +52,15 @@ struct ProxOp {
   int* err;            // device flag set when a bounded wait gives up (never expected)
   int defer_zero = 0;  // 1: the apply kernel leaves blocks with r_a = 0 unwritten; the fused
                        // FFT that follows in the same iteration zero-fills them as it loads
+  float2* vwide = nullptr;  // 64 < n <= 128: per-CTA eigenvector scratch of the wide Jacobi kernel,
+  int vwide_ctas = 0;       // vwide_ctas * wide_v_stride() float2
 };
+
+// Widest Casorati column count of the prox kernels, and the per-CTA eigenvector scratch the
+// wide (64 < n <= 128) Jacobi kernel needs, in float2.
+constexpr int kProxMaxN = 128;
+__host__ __device__ inline long long wide_v_stride() { return (long long)kProxMaxN * (kProxMaxN + 1); }
+int wide_jacobi_ctas();   // CTAs of the wide Jacobi kernel on the current device
 
 // Kept eigenvectors per block that the warp eigen kernel hands to the apply kernel.
 constexpr int kFacCols = 8;
@@ -161,6 +172,9 @@ struct llr_ctx {
   int* d_blk_ra;            // per-block kept count of the split prox path + queue counter
   int* d_err;               // device error flag of the prox kernels
   int ph_uniform;           // all volumes share the image-domain phase tables
+  float2* d_vwide;          // eigenvector scratch of the wide (64 < nq <= 128) Jacobi kernel
+  int vwide_ctas;
+  std::vector<int> phase_off;   // overlapping blocks: 3 offsets per phase (empty: non-overlapping)
   float2* d_wavelet_work;
   size_t wavelet_work_elems;
   llr::WaveletPlan wplan;

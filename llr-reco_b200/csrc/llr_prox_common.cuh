@@ -37,6 +37,7 @@ __device__ __forceinline__ void block_shift(const BlockSource& s, int* sh) {
   } else {
     sh[0] = s.sx; sh[1] = s.sy; sh[2] = s.sz;
   }
+  sh[0] += s.ox; sh[1] += s.oy; sh[2] += s.oz;
 }
 
 // Voxel coordinates of row r of block `blk`.  Rows are ordered y fastest, then z, then x, and
@@ -97,7 +98,9 @@ __device__ void scatter_block(const BlockSource& s, long long blk, const int* sh
     block_row_coord(s, blk, sh, r, ix, iy, iz);
     float2 v = cscale(Cs[q * ldc + r], s.store_scale);
     if (s.store_phase) v = cmul(v, phase_at(s.ph, s.g, q, ix, iy, iz));
-    s.data[planar_index(s.g, ix, iy, iz, q)] = v;
+    float2* dst = (s.out ? s.out : s.data) + planar_index(s.g, ix, iy, iz, q);
+    if (s.accumulate) v = cadd(v, *dst);
+    *dst = v;
   }
 }
 

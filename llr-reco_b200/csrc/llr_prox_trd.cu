@@ -464,7 +464,25 @@ __device__ __forceinline__ void store_elem(const BlockSource& s, long long base,
       v = cmul(v, p);
     }
   }
-  s.data[base + (long long)rt.off + (long long)q * qstride] = v;
+  float2* dst = (s.out ? s.out : s.data) + base + (long long)rt.off + (long long)q * qstride;
+  if (s.accumulate) v = cadd(v, *dst);
+  *dst = v;
+}
+
+// Identity result of a block written to a separate output: every element loaded (with the
+// load transform) and stored (with the store transform).
+__device__ void copy_rows(const BlockSource& s, long long base, const RowTab* rows, const float2* rowph, int m, int n,
+                          long long qstride) {
+  for (int r = threadIdx.x; r < m; r += blockDim.x) {
+    const RowTab rt = rows[r];
+    for (int k0 = 0; k0 < n; k0 += 8) {
+      float2 c[8];
+      load_row_batch<8>(s, base, rt, rowph, r, k0, n, qstride, c);
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        if (k0 + u < n) store_elem(s, base, rt, rowph, r, k0 + u, qstride, c[u]);
+    }
+  }
 }
 
 struct TrdLayout {
@@ -695,15 +713,17 @@ __global__ void __launch_bounds__(kLlrThreads, 2) llr_prox_trd_kernel(BlockSourc
     }
     tridiag_setup<NPMAX>(trd, n, op.mode, op.rank, op.lambda, misc);
     const int ra = misc->ra, nb = misc->n_below;
-    if (ra == n && op.mode == LLR_PROX_HARD_RANK) {
+    if (ra == n && op.mode == LLR_PROX_HARD_RANK) {   // rank >= n: identity
+      if (src.out) copy_rows(src, base, rows, rowph, m, n, qstride);
       __syncthreads();
-      continue;  // rank >= n: identity, nothing to write
+      continue;
     }
     if (ra == 0) {
-      for (int idx = tid; idx < m * n; idx += blockDim.x) {
-        const int q = idx / m, r = idx - q * m;
-        store_elem(src, base, rows[r], rowph, r, q, qstride, make_float2(0.f, 0.f));
-      }
+      if (!src.accumulate)
+        for (int idx = tid; idx < m * n; idx += blockDim.x) {
+          const int q = idx / m, r = idx - q * m;
+          store_elem(src, base, rows[r], rowph, r, q, qstride, make_float2(0.f, 0.f));
+        }
       __syncthreads();
       continue;
     }
@@ -854,9 +874,10 @@ __global__ void __launch_bounds__(kEigThreads, 4) llr_eig_apply_kernel(BlockSour
       ra = misc->ra;
       nb = misc->n_below;
     }
-    if (ra == n && op.mode == LLR_PROX_HARD_RANK) {
+    const bool identity = ra == n && op.mode == LLR_PROX_HARD_RANK;   // rank >= n
+    if (identity && !src.out) {
       __syncthreads();
-      continue;  // rank >= n: identity, nothing to write
+      continue;
     }
     // row tables (only the apply needs them here)
     for (int r = tid; r < m; r += blockDim.x) {
@@ -877,11 +898,17 @@ __global__ void __launch_bounds__(kEigThreads, 4) llr_eig_apply_kernel(BlockSour
       rows[r] = rt;
     }
     __syncthreads();
+    if (identity) {
+      copy_rows(src, base, rows, rowph, m, n, qstride);
+      __syncthreads();
+      continue;
+    }
     if (ra == 0) {
-      for (int idx = tid; idx < m * n; idx += blockDim.x) {
-        const int q = idx / m, r = idx - q * m;
-        store_elem(src, base, rows[r], rowph, r, q, qstride, make_float2(0.f, 0.f));
-      }
+      if (!src.accumulate)
+        for (int idx = tid; idx < m * n; idx += blockDim.x) {
+          const int q = idx / m, r = idx - q * m;
+          store_elem(src, base, rows[r], rowph, r, q, qstride, make_float2(0.f, 0.f));
+        }
       __syncthreads();
       continue;
     }
@@ -1024,7 +1051,10 @@ __global__ void __launch_bounds__(kApplyThreads, 3) llr_apply_kernel(BlockSource
   const int sh[3] = {sh_s[0], sh_s[1], sh_s[2]};
   for (long long blk = blockIdx.x; blk < src.nblocks; blk += gridDim.x) {
     const int ra = op.blk_ra[blk];
-    if (ra < 0 || (ra == 0 && op.defer_zero)) continue;   // uniform over the CTA
+    // uniform over the CTA: fallback blocks (-1) belong to the Jacobi kernel; identity blocks (-2)
+    // stay in place unless the result goes to a separate output; zero blocks need no store when
+    // deferred to the fused FFT or accumulated
+    if (ra == -1 || (ra == -2 && !src.out) || (ra == 0 && (op.defer_zero || src.accumulate))) continue;
     const long long base = src.kind == 1 ? 0 : blk * (long long)m * n;
     for (int r = tid; r < m; r += blockDim.x) {
       RowTab rt;
@@ -1049,9 +1079,11 @@ __global__ void __launch_bounds__(kApplyThreads, 3) llr_apply_kernel(BlockSource
       if (tid < kFacCols) g[tid] = F[n * kFacCols + tid].x;
     }
     __syncthreads();
-    if (ra == 0) {   // every singular value below the threshold: the block becomes zero
+    if (ra == -2) {
+      copy_rows(src, base, rows, rowph, m, n, qstride);
+    } else if (ra == 0) {   // every singular value below the threshold: the block becomes zero
       for (int r = tid; r < m; r += blockDim.x) {
-        float2* rowp = src.data + base + (long long)rows[r].off;
+        float2* rowp = (src.out ? src.out : src.data) + base + (long long)rows[r].off;
         for (int q = 0; q < n; ++q) rowp[(long long)q * qstride] = make_float2(0.f, 0.f);
       }
     } else if (refine) {
@@ -1067,6 +1099,128 @@ __global__ void __launch_bounds__(kApplyThreads, 3) llr_apply_kernel(BlockSource
     }
     __syncthreads();
   }
+}
+
+// =======================================================================================
+// Casorati matrices with 64 < n <= 128 columns that the split path cannot finish (more kept
+// components than the warp eigen kernel holds, or a failed residual check), and every block
+// at that width for the Jacobi solver and the block statistics: Gram matrix over staged row
+// chunks into shared memory, cyclic Jacobi with the eigenvectors in a per-CTA global scratch
+// (L2-resident), W = V diag(g) V^H, C' = C W streamed over row chunks.  One CTA per SM.
+// =======================================================================================
+constexpr int kWideTG = 8;
+constexpr int kWideRows = 32;
+
+struct WideLayout {
+  TrdLayout t;     // rc / ldch / ksplit / np and the row-table offsets for gram_block
+  size_t off_rot, off_pair, off_ev, off_g, off_act, off_A, total;
+};
+
+inline WideLayout make_wide_layout(int m, int n) {
+  WideLayout W;
+  TrdLayout& L = W.t;
+  const int nt = (n + kWideTG - 1) / kWideTG;
+  L.np = nt * kWideTG;
+  L.ksplit = 1;
+  L.rc = std::min(kWideRows, m);
+  L.ldch = (L.rc & 1) ? L.rc : L.rc + 1;
+  size_t off = 256;   // Misc
+  W.off_rot = off; off = align16(off + sizeof(float4) * (kProxMaxN / 2));
+  W.off_pair = off; off = align16(off + sizeof(int2) * (kProxMaxN / 2));
+  W.off_ev = off; off = align16(off + sizeof(float) * kProxMaxN);
+  W.off_g = off; off = align16(off + sizeof(float) * kProxMaxN);
+  W.off_act = off; off = align16(off + sizeof(int) * kProxMaxN);
+  L.off_row = off; off = align16(off + sizeof(RowTab) * (size_t)m);
+  L.off_rowph = off; off = align16(off + sizeof(float2) * (size_t)m);
+  W.off_A = off; off = align16(off + sizeof(float2) * kProxMaxN * (kProxMaxN + 1));
+  L.off_C = off; off = align16(off + sizeof(float2) * (size_t)n * L.ldch);
+  L.total = W.total = off;
+  return W;
+}
+
+__global__ void __launch_bounds__(kLlrThreads, 1) llr_prox_wide_kernel(BlockSource src, ProxOp op, WideLayout W) {
+  constexpr int NP = kProxMaxN, lda = NP + 1;
+  extern __shared__ __align__(16) unsigned char smem[];
+  Misc* misc = reinterpret_cast<Misc*>(smem);
+  float4* rot = reinterpret_cast<float4*>(smem + W.off_rot);
+  int2* pairs = reinterpret_cast<int2*>(smem + W.off_pair);
+  float* ev = reinterpret_cast<float*>(smem + W.off_ev);
+  float* g = reinterpret_cast<float*>(smem + W.off_g);
+  int* act = reinterpret_cast<int*>(smem + W.off_act);
+  RowTab* rows = reinterpret_cast<RowTab*>(smem + W.t.off_row);
+  float2* rowph = reinterpret_cast<float2*>(smem + W.t.off_rowph);
+  float2* A = reinterpret_cast<float2*>(smem + W.off_A);
+  float2* Cch = reinterpret_cast<float2*>(smem + W.t.off_C);
+  float2* V = op.vwide + (long long)blockIdx.x * wide_v_stride();
+  const int m = op.m, n = op.n, tid = threadIdx.x;
+  const long long qstride = src.kind == 1 ? src.g.V : (long long)m;
+  if (tid == 0) block_shift(src, misc->shift);
+  __syncthreads();
+  const int sh[3] = {misc->shift[0], misc->shift[1], misc->shift[2]};
+  const long long count = src.blk_list ? (long long)*src.blk_count : src.nblocks;
+  for (long long i = blockIdx.x; i < count; i += gridDim.x) {
+    const long long blk = src.blk_list ? (long long)src.blk_list[i] : i;
+    const long long base = src.kind == 1 ? 0 : blk * (long long)m * n;
+    for (int k = tid; k < NP * lda; k += blockDim.x) A[k] = make_float2(0.f, 0.f);
+    gram_block<NP, kWideTG>(src, W.t, m, n, blk, base, qstride, sh, rows, rowph, Cch,
+                            [&](int a, int b, float2 v) { A[a * lda + b] = v; });
+    jacobi<NP>(A, V, n, rot, pairs, misc, 20);
+    if (op.block_stat) {
+      if (tid == 0) {
+        float mx = 0.f;
+        for (int k = 0; k < n; ++k) mx = fmaxf(mx, A[k * lda + k].x);
+        op.block_stat[blk] = mx;
+      }
+      __syncthreads();
+      continue;
+    }
+    singular_map(A, lda, n, op.mode, op.rank, op.lambda, ev, g, act, misc);
+    const int na = misc->n_active;
+    const bool identity = na == n && op.mode == LLR_PROX_HARD_RANK;
+    if (identity && !src.out) {
+      __syncthreads();
+      continue;
+    }
+    if (na == 0 && src.accumulate) {
+      __syncthreads();
+      continue;
+    }
+    if (!identity) form_W(A, V, lda, n, g, act, na);
+    for (int c0 = 0; c0 < m; c0 += W.t.rc) {
+      const int rc = min(W.t.rc, m - c0);
+      for (int e = tid; e < rc * n; e += blockDim.x) {
+        const int q = e / rc, rr = e - q * rc, r = c0 + rr;
+        const RowTab rt = rows[r];
+        float2 x = src.data[base + (long long)rt.off + (long long)q * qstride];
+        if (src.kind == 1) {
+          const float2 p = src.ph_uniform ? rowph[r] : phase_at(src.ph, src.g, q, rt.cx, rt.cyz & 0xffff, rt.cyz >> 16);
+          x = cscale(cmul_bc(x, p), src.load_scale);
+        }
+        Cch[q * W.t.ldch + rr] = x;
+      }
+      __syncthreads();
+      if (!identity) apply_W<NP, kWideTG>(Cch, W.t.ldch, rc, n, A);
+      for (int e = tid; e < rc * n; e += blockDim.x) {
+        const int q = e / rc, rr = e - q * rc, r = c0 + rr;
+        store_elem(src, base, rows[r], rowph, r, q, qstride, Cch[q * W.t.ldch + rr]);
+      }
+      __syncthreads();
+    }
+  }
+}
+
+int launch_prox_wide(const BlockSource& src, const ProxOp& op, cudaStream_t stream) {
+  if (!op.vwide || op.vwide_ctas < 1) return set_error(LLR_ERR_INVALID, "wide prox needs its eigenvector scratch");
+  const WideLayout W = make_wide_layout(op.m, op.n);
+  if (W.total > 227 * 1024)
+    return set_error(LLR_ERR_UNSUPPORTED, "Casorati %dx%d needs %zu B of shared memory", op.m, op.n, W.total);
+  LLR_CUDA_TRY(cudaFuncSetAttribute(llr_prox_wide_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)W.total));
+  const long long grid = std::min<long long>(src.blk_list ? op.vwide_ctas : src.nblocks, op.vwide_ctas);
+  if (grid < 1) return LLR_OK;
+  note_launch();
+  llr_prox_wide_kernel<<<(unsigned)grid, kLlrThreads, W.total, stream>>>(src, op, W);
+  LLR_CUDA_TRY(cudaGetLastError());
+  return LLR_OK;
 }
 
 int launch_apply(const BlockSource& src, const ProxOp& op, cudaStream_t stream) {
@@ -1092,7 +1246,12 @@ int launch_split_instance(const BlockSource& src, const ProxOp& op, cudaStream_t
   if (op.gram_mode == 0 && llr_gram_tc_supported(op.m, op.n)) {
     LLR_TRY(launch_llr_gram_tc(src, op, stream));
   } else {
+    // the Gram kernel uses the row tables and the chunk buffer only
     TrdLayout L = make_trd_layout<NPMAX, TG>(op.m, op.n);
+    const size_t chunk = sizeof(float2) * (size_t)op.n * L.ldch;
+    const size_t scr = L.ksplit > 1 ? sizeof(float2) * (size_t)L.ksplit * L.np * L.np : 0;
+    L.off_C = L.off_A;
+    L.total = align16(L.off_C + std::max(chunk, scr));
     auto kern = llr_gram_kernel<NPMAX, TG>;
     LLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total));
     LLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
@@ -1124,7 +1283,15 @@ int launch_split_instance(const BlockSource& src, const ProxOp& op, cudaStream_t
 
 }  // namespace
 
+int wide_jacobi_ctas() {
+  int dev = 0, nsm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return 148;
+  return nsm;
+}
+
 bool llr_prox_supported(int m, int n) {
+  if (n > 64 && n <= kProxMaxN && m >= 1 && m <= 65535) return make_wide_layout(m, n).total <= 227 * 1024;
   if (m < 1 || n < 1 || n > 64 || m > 65535) return false;
   size_t t;
   if (n <= 16) t = make_trd_layout<16, 2>(m, n).total;
@@ -1138,12 +1305,19 @@ bool llr_prox_supported(int m, int n) {
 int launch_llr_prox(const BlockSource& src, const ProxOp& op, cudaStream_t stream) {
   if (op.n < 1 || op.m < 1) return set_error(LLR_ERR_INVALID, "empty Casorati matrix %dx%d", op.m, op.n);
   if (src.nblocks == 0) return LLR_OK;
+  if (op.n > 64) {   // wide matrices (64 < n <= 128): the wide Jacobi kernel over every block
+    if (op.n > kProxMaxN)
+      return set_error(LLR_ERR_UNSUPPORTED, "Casorati column count %d > %d is not supported", op.n, kProxMaxN);
+    if (!op.vwide)
+      return set_error(LLR_ERR_UNSUPPORTED, "Casorati column count %d > 64 needs the wide-kernel scratch of a "
+                                            "context or of an allocating entry point", op.n);
+    return launch_prox_wide(src, op, stream);
+  }
   if (op.eig_solver == 1) return launch_llr_prox_jacobi(src, op, stream);
   if (!op.block_stat && !op.fb_list)
     return set_error(LLR_ERR_INVALID, "tridiagonal prox needs a fallback block list");
   if (op.fb_count) LLR_CUDA_TRY(cudaMemsetAsync(op.fb_count, 0, sizeof(int), stream));
   int st;
-  if (op.n > 64) return set_error(LLR_ERR_UNSUPPORTED, "Casorati column count %d > 64 is not supported", op.n);
   if (op.gram) {  // split path: Gram kernel + eigen/apply kernel through the scratch buffer
     if (op.n <= 16) st = launch_split_instance<16, 2>(src, op, stream);
     else if (op.n <= 32) st = launch_split_instance<32, 2>(src, op, stream);

@@ -619,6 +619,7 @@ class ReconConfig:
     lin_ksp: Optional[np.ndarray] = None
     lin_img: Optional[np.ndarray] = None
     wavelet_space: str = "image"  # with a subspace: "image" (lib.rs:302-309) | "coeffs" (srank volumes)
+    block_stride: Optional[tuple] = None   # None / == block size: non-overlapping grid (block.rs:112-133)
 
 
 def llr_prox_coeffs(x: np.ndarray, cfg: ReconConfig, shift) -> np.ndarray:
@@ -636,7 +637,28 @@ def llr_prox_coeffs(x: np.ndarray, cfg: ReconConfig, shift) -> np.ndarray:
 
 
 def llr_prox(x: np.ndarray, cfg: ReconConfig, shift) -> np.ndarray:
-    """lib.rs:270-296: lift every block, low-rank it, un-lift (non-overlapping grid)."""
+    """lib.rs:270-296: lift every block, low-rank it, un-lift.
+
+    With ``cfg.block_stride`` s < b (overlapping blocks every s voxels, b % s == 0, the blocks
+    tiling the volume) every voxel becomes the mean of the outputs of the (b/s)^3 blocks that
+    cover it: the strided grid splits into (b/s)^3 non-overlapping tilings, at the shift plus an
+    offset in {0, s, ..., b - s} per axis, and the result is the mean of their prox outputs."""
+    bs = tuple(cfg.block_size)
+    st = tuple(cfg.block_stride) if cfg.block_stride is not None else bs
+    if st != bs:
+        per = [b // s if 0 < s < b else 1 for b, s in zip(bs, st)]
+        offs = [[k * s for k in range(p)] if p > 1 else [0] for p, s in zip(per, st)]
+        acc = np.zeros_like(x)
+        for oz in offs[2]:
+            for oy in offs[1]:
+                for ox in offs[0]:
+                    acc += _llr_prox_tiling(x, cfg, (shift[0] + ox, shift[1] + oy, shift[2] + oz))
+        return np.asfortranarray(acc / float(np.prod(per)))
+    return _llr_prox_tiling(x, cfg, shift)
+
+
+def _llr_prox_tiling(x: np.ndarray, cfg: ReconConfig, shift) -> np.ndarray:
+    """One non-overlapping tiling at ``shift`` (the reference's grid)."""
     nx, ny, nz, nq = x.shape
     g = grid_dim((nx, ny, nz), cfg.block_size)
     nb = int(np.prod(g))

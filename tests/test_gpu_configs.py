@@ -105,3 +105,48 @@ def test_c3_coefficient_wavelet(gpu):
     assert np.all(np.isfinite(hist))
     assert rel_err(gx, ox) < TOL, rel_err(gx, ox)
     np.testing.assert_allclose(hist, oh, rtol=TOL)
+
+
+def test_c5_shape_class_overlapping_blocks(gpu):
+    """Config-5 shape class: 106 volumes (6 b0 + 100 over b = 1000 / 2000 / 3000), 12x sampling,
+    8^3 blocks at stride 4 (Casorati 512 x 106, each voxel the mean of its 8 block outputs),
+    random shift per iteration, soft threshold 0.02 sigma_max; a 32^3 volume, 2 iterations."""
+    vol, bs, st, n_iter = (32, 32, 32), (8, 8, 8), (4, 4, 4), 2
+    d = make_dataset(vol, [(0, 6), (1000, 34), (2000, 33), (3000, 33)], 12.0, 2, centre=8, mask_fn=O.vd_mask)
+    y = d.y
+    assert y.shape[3] == 106
+    ocfg = O.ReconConfig(block_size=bs, mode="soft", seed=19, block_stride=st)
+    x0 = O.zero_filled(y.astype(np.complex128), ocfg)
+    ocfg.lam = 0.02 * O.sigma_max(x0, bs)
+    p = ReconParams(vol_size=vol, nq=106, block_size=bs, prox_mode=L.LLR_PROX_SOFT_THRESH, lam=ocfg.lam, seed=19,
+                    block_stride=st)
+    with ReconContext(p) as ctx:
+        ctx.upload_kspace(y)
+        ctx.init_zero_filled()
+        hist = ctx.iterate(n_iter)
+        gx = ctx.download_image()
+    ox, oh = O.recon(y.astype(np.complex128), ocfg, n_iter, x0=x0)
+    assert np.all(np.isfinite(hist))
+    assert rel_err(gx, ox) < TOL, rel_err(gx, ox)
+    np.testing.assert_allclose(hist, oh, rtol=TOL)
+
+
+@pytest.mark.parametrize("nq,stride", [(17, (4, 4, 4)), (80, None), (20, (2, 4, 8))])
+def test_overlap_and_wide_paths(gpu, nq, stride):
+    """Overlapping blocks with the split prox path (17 volumes; anisotropic strides 2 / 4 / 8, i.e.
+    8 phases of 4 x 2 x 1) and the wide Jacobi kernel on a non-overlapping grid (80 volumes)."""
+    vol, bs = (24, 24, 16), (8, 8, 8)
+    d = make_dataset(vol, [(0, 1), (1000, nq - 1)], 4.0, 3, centre=6, mask_fn=O.vd_mask)
+    ocfg = O.ReconConfig(block_size=bs, mode="soft", seed=23, block_stride=stride)
+    x0 = O.zero_filled(d.y.astype(np.complex128), ocfg)
+    ocfg.lam = 0.02 * O.sigma_max(x0, bs)
+    p = ReconParams(vol_size=vol, nq=nq, block_size=bs, prox_mode=L.LLR_PROX_SOFT_THRESH, lam=ocfg.lam, seed=23,
+                    block_stride=stride)
+    with ReconContext(p) as ctx:
+        ctx.upload_kspace(d.y)
+        ctx.init_zero_filled()
+        hist = ctx.iterate(3)
+        gx = ctx.download_image()
+    ox, oh = O.recon(d.y.astype(np.complex128), ocfg, 3, x0=x0)
+    assert rel_err(gx, ox) < TOL, rel_err(gx, ox)
+    np.testing.assert_allclose(hist, oh, rtol=TOL)

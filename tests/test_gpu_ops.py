@@ -63,7 +63,8 @@ def test_lift_unlift_match_oracle_exactly(gpu, vol, bs, shift):
     np.testing.assert_array_equal(zero, ref.reshape(-1, order="F"))
 
 
-@pytest.mark.parametrize("m,n,rank", [(64, 9, 3), (216, 61, 6), (512, 17, 5), (100, 33, 1), (20, 10, 10)])
+@pytest.mark.parametrize("m,n,rank", [(64, 9, 3), (216, 61, 6), (512, 17, 5), (100, 33, 1), (20, 10, 10),
+                                    (512, 106, 6), (150, 128, 20), (200, 65, 65)])
 def test_hard_rank_batch_matches_oracle(gpu, m, n, rank):
     rng = np.random.default_rng(12)
     batch = 7
@@ -78,7 +79,7 @@ def test_hard_rank_batch_matches_oracle(gpu, m, n, rank):
     assert rel_err(buf.reshape(m, n, batch, order="F"), exp) < 5e-5
 
 
-@pytest.mark.parametrize("m,n", [(64, 9), (216, 61), (512, 17), (40, 40), (512, 7)])
+@pytest.mark.parametrize("m,n", [(64, 9), (216, 61), (512, 17), (40, 40), (512, 7), (512, 106), (128, 100)])
 def test_soft_threshold_batch_matches_oracle(gpu, m, n):
     rng = np.random.default_rng(13)
     batch = 9

@@ -261,3 +261,27 @@ def test_dti_fit_recovers_noise_free_tensor():
     r = O.dti_fit(dwi, b0, b[b > 0], g[b > 0])
     np.testing.assert_allclose([r["e1"][0], r["e2"][0], r["e3"][0]], [1.7e-3, 0.5e-3, 0.3e-3], rtol=1e-9)
     np.testing.assert_allclose(r["md"][0], 2.5e-3 / 3, rtol=1e-9)
+
+
+def test_overlapping_prox_is_the_mean_over_covering_blocks():
+    """The oracle's overlapping prox (phases of non-overlapping tilings) equals the direct
+    definition: every block of the stride-s grid (lift_data_set with a stride) low-ranked, its
+    output added to every voxel it covers, divided by the number of covering blocks."""
+    rng = np.random.default_rng(5)
+    vol, bs, st, nq = (16, 8, 16), (8, 4, 8), (4, 2, 8), 5
+    x = np.asfortranarray((rng.standard_normal(vol + (nq,)) + 1j * rng.standard_normal(vol + (nq,))))
+    shift = (3, 5, 1)
+    cfg = O.ReconConfig(block_size=bs, mode="soft", lam=1.5, block_stride=st)
+    got = O.llr_prox(x, cfg, shift)
+    g = O.grid_dim_strided(vol, bs, st)
+    nb = int(np.prod(g))
+    mats = O.low_rank_soft(O.lift_data_set(x, bs, shift, 0, nb, stride=st), 1.5)
+    acc = np.zeros((int(np.prod(vol)), nq), dtype=complex)
+    cnt = np.zeros(int(np.prod(vol)))
+    for b in range(nb):
+        idx = O._block_voxel_index(vol, bs, O.block_coord(b, vol, bs, shift, st))
+        acc[idx] += mats[:, :, b]
+        cnt[idx] += 1
+    assert np.all(cnt == 2 * 2 * 1)
+    exp = (acc / cnt[:, None]).reshape(vol + (nq,), order="F")
+    np.testing.assert_allclose(got, exp, rtol=1e-12, atol=1e-12)
