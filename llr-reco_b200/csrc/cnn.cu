@@ -1,7 +1,8 @@
 // Learned warm start: a small 3-D residual CNN (conv3d 3x3x3, zero padding, ReLU between
 // layers, out = in + net(in)) with hand-written forward, backward-data and backward-weight
 // kernels, mean-squared-error loss and Adam.  BF16 weights feed the convolutions with FP32
-// accumulation; the optimizer keeps FP32 master weights.
+// accumulation (forward and backward-data on the tensor cores, tcgen05 TF32 with the
+// activations split hi + lo); the optimizer keeps FP32 master weights.
 //
 // Activations are channels-last FP32, voxel v = x + nx (y + ny z) (the reference image order,
 // x fastest).  Forward:  y[v][co] = b[co] + sum_{tap, ci} W[tap][ci][co] x[v + d(tap) - 1][ci],
@@ -20,6 +21,7 @@
 
 #include "llr_common.cuh"
 #include "llr_internal.h"
+#include "llr_umma.cuh"
 
 struct llr_cnn {
   int device;
@@ -44,23 +46,12 @@ struct llr_cnn {
   long long part_cap;
   double* d_loss;                        // loss partial sums
   int loss_cap;
+  int* d_err;                            // set by a conv kernel whose bounded tensor-core wait ran out
 };
 
 namespace llr {
 
 namespace {
-
-constexpr int kTX = 8, kTY = 8, kTZ = 4;                      // output tile
-constexpr int kHX = kTX + 2, kHY = kTY + 2, kHZ = kTZ + 2;     // input halo tile
-constexpr int kHV = kHX * kHY * kHZ;
-constexpr int kTV = kTX * kTY * kTZ;
-constexpr int kConvThreads = 128;                              // two voxels (z, z + 2) per thread
-constexpr int kWgThreads = 288;
-
-__host__ __device__ constexpr int odd_pitch(int c) { return c | 1; }
-__host__ __device__ constexpr int pad4(int c) { return (c + 3) & ~3; }
-
-__device__ __forceinline__ float bf16_to_f32(uint16_t h) { return __uint_as_float((uint32_t)h << 16); }
 
 __host__ __device__ __forceinline__ uint16_t f32_to_bf16(float f) {
 #ifdef __CUDA_ARCH__
@@ -74,171 +65,385 @@ __host__ __device__ __forceinline__ uint16_t f32_to_bf16(float f) {
   return (uint16_t)(u >> 16);
 }
 
-struct TileGeo {
-  int nx, ny, nz, tx, ty;   // volume and tile counts along x, y
-  __device__ void origin(long long tile, int& ox, int& oy, int& oz) const {
-    const int ix = (int)(tile % tx);
-    const long long r = tile / tx;
-    const int iy = (int)(r % ty);
-    const int iz = (int)(r / ty);
-    ox = ix * kTX; oy = iy * kTY; oz = iz * kTZ;
-  }
+// ---------------------------------------------------------------------------------------
+// conv3d as an implicit GEMM on the tensor cores (tcgen05, TF32 with FP32 accumulation in
+// tensor memory).  A CTA owns tiles of 128 output voxels (8 x 4 x 4); per tile the halo
+// (10 x 6 x 6 voxels, all input channels) is staged once in shared memory, then for each of
+// the 27 taps the 128 x CIN operand (the tap-shifted voxels) is split into TF32 hi + lo planes
+// in the 128-byte swizzled K-major layout and multiplied with that tap's weights (BF16, exact
+// in TF32; all 27 taps resident in shared memory, N = COUT padded to 16 / 32, K = CIN padded
+// to 32).  D[voxel][co] += hi W + lo W keeps FP32-level accuracy (the split error of x is
+// ~2^-22 relative).  Two operand buffers: the planes of tap t + 1 are written while the tensor
+// core works on tap t; one elected thread issues the MMAs and commits them to mbarriers with
+// bounded waits.  Epilogue: tcgen05.ld of the accumulator, bias, ReLU, residual, store.
+// ---------------------------------------------------------------------------------------
+constexpr int kCvThreads = 256;
+constexpr int kCvTX = 8, kCvTY = 4, kCvTZ = 4;                  // 128 output voxels per tile
+constexpr int kCvHX = kCvTX + 2, kCvHY = kCvTY + 2, kCvHZ = kCvTZ + 2;
+constexpr int kCvHV = kCvHX * kCvHY * kCvHZ;
+constexpr int kCvPlane = 128 * 128;                              // one 128 x 32 TF32 operand plane (bytes)
+
+__host__ __device__ constexpr int cv_np(int cout) { return cout <= 16 ? 16 : 32; }
+
+template <int CIN, int COUT>
+struct CvLayout {
+  static constexpr int NP = cv_np(COUT);
+  static constexpr int HP = CIN | 1;                               // halo channel pitch (odd)
+  static constexpr size_t off_hdr = 0;                             // 3 mbarriers + TMEM address
+  static constexpr size_t off_w = 1024;                            // 27 tap blocks of NP x 128 B
+  static constexpr size_t off_a = off_w + (size_t)27 * NP * 128;   // 2 buffers x (hi, lo)
+  static constexpr size_t off_halo = off_a + (size_t)4 * kCvPlane;
+  static constexpr size_t total = off_halo + sizeof(float) * (size_t)kCvHV * HP;
 };
 
-// halo tile of C channels -> s[hv * CP + c], zero outside the volume
-template <int C>
-__device__ __forceinline__ void load_halo(const float* __restrict__ x, float* s, const TileGeo& G, int ox, int oy,
-                                          int oz) {
-  constexpr int CP = odd_pitch(C);
-  for (int i = threadIdx.x; i < kHV * C; i += blockDim.x) {
-    const int hv = i / C, c = i - hv * C;
-    const int hx = hv % kHX, hy = (hv / kHX) % kHY, hz = hv / (kHX * kHY);
-    const int gx = ox + hx - 1, gy = oy + hy - 1, gz = oz + hz - 1;
-    float v = 0.f;
-    if (gx >= 0 && gx < G.nx && gy >= 0 && gy < G.ny && gz >= 0 && gz < G.nz)
-      v = x[((long long)gx + (long long)G.nx * (gy + (long long)G.ny * gz)) * C + c];
-    s[hv * CP + c] = v;
-  }
-}
+struct CvGeo {
+  int nx, ny, nz, tx, ty;
+  long long ntiles;
+};
 
-// y = [add +] act(b + conv(x, W)); W in BF16 [27][CIN][COUT].
 template <int CIN, int COUT>
-__global__ void __launch_bounds__(kConvThreads) conv3d_kernel(const float* __restrict__ x, const uint16_t* __restrict__ wb,
-                                                              const float* __restrict__ bias, const float* __restrict__ add,
-                                                              float* __restrict__ y, TileGeo G, int relu) {
-  constexpr int CP = odd_pitch(CIN), COP = pad4(COUT);
-  extern __shared__ __align__(16) float smem_f[];
-  float* s_w = smem_f;                    // [27][CIN][COP]
-  float* s_in = smem_f + 27 * CIN * COP;  // [kHV][CP]
-  for (int i = threadIdx.x; i < 27 * CIN * COP; i += blockDim.x) {
-    const int co = i % COP, tc = i / COP;
-    s_w[i] = co < COUT ? bf16_to_f32(wb[tc * COUT + co]) : 0.f;
+__global__ void __launch_bounds__(kCvThreads, 1) conv3d_tc_kernel(const float* __restrict__ x,
+                                                                  const uint16_t* __restrict__ wb,
+                                                                  const float* __restrict__ bias,
+                                                                  const float* __restrict__ add, float* __restrict__ y,
+                                                                  CvGeo G, int relu, int* err) {
+  using Lay = CvLayout<CIN, COUT>;
+  constexpr int NP = Lay::NP, HP = Lay::HP;
+  constexpr uint32_t idesc = umma_idesc_tf32(128, NP);
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned long long* mbar = reinterpret_cast<unsigned long long*>(smem + Lay::off_hdr);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + Lay::off_hdr + 32);
+  unsigned char* wsm = smem + Lay::off_w;
+  unsigned char* asm_ = smem + Lay::off_a;
+  float* halo = reinterpret_cast<float*>(smem + Lay::off_halo);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(32u));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
-  int ox, oy, oz;
-  G.origin(blockIdx.x, ox, oy, oz);
-  load_halo<CIN>(x, s_in, G, ox, oy, oz);
+  if (tid == 0) {
+    for (int b = 0; b < 3; ++b) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[b])));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  // operand planes and weight blocks start zeroed (K padding CIN..31, N padding COUT..NP-1)
+  for (int i = tid; i < (int)((Lay::off_halo - Lay::off_w) / 16); i += kCvThreads)
+    reinterpret_cast<float4*>(wsm)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
   __syncthreads();
-  const int t = threadIdx.x;
-  const int lx = t & 7, ly = (t >> 3) & 7, lz = t >> 6;
-  float acc0[COP], acc1[COP];
-#pragma unroll
-  for (int c = 0; c < COP; ++c) {
-    const float b0 = (bias && c < COUT) ? bias[c] : 0.f;
-    acc0[c] = b0;
-    acc1[c] = b0;
+  for (int i = tid; i < 27 * CIN * COUT; i += kCvThreads) {   // W[tap][ci][co] -> tap block, row co, column ci
+    const int co = i % COUT, r = i / COUT, ci = r % CIN, tap = r / CIN;
+    *reinterpret_cast<uint32_t*>(wsm + (size_t)tap * NP * 128 + op_offset(co, ci)) = (uint32_t)wb[i] << 16;
   }
-  for (int dz = 0; dz < 3; ++dz)
-    for (int dy = 0; dy < 3; ++dy)
-#pragma unroll 1
-      for (int dx = 0; dx < 3; ++dx) {
-        const int hv0 = ((lz + dz) * kHY + (ly + dy)) * kHX + lx + dx;
-        const float* p0 = s_in + hv0 * CP;
-        const float* p1 = p0 + 2 * kHX * kHY * CP;
-        const float* pw = s_w + (dx + 3 * (dy + 3 * dz)) * CIN * COP;
-#pragma unroll 4
-        for (int ci = 0; ci < CIN; ++ci) {
-          const float xa = p0[ci], xb = p1[ci];
-          const float4* w4 = reinterpret_cast<const float4*>(pw + ci * COP);
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = *tmem_slot;
+  uint32_t phase[3] = {0u, 0u, 0u};
+  bool used[2] = {false, false};
+  bool failed = false;
+  int gpar = 0;
+
+  for (long long tile = blockIdx.x; tile < G.ntiles && !failed; tile += gridDim.x) {
+    const int ox = (int)(tile % G.tx) * kCvTX;
+    const long long rt = tile / G.tx;
+    const int oy = (int)(rt % G.ty) * kCvTY, oz = (int)(rt / G.ty) * kCvTZ;
+    for (int i = tid; i < kCvHV * CIN; i += kCvThreads) {
+      const int hv = i / CIN, c = i - hv * CIN;
+      const int hx = hv % kCvHX, hy = (hv / kCvHX) % kCvHY, hz = hv / (kCvHX * kCvHY);
+      const int gx = ox + hx - 1, gy = oy + hy - 1, gz = oz + hz - 1;
+      float v = 0.f;
+      if (gx >= 0 && gx < G.nx && gy >= 0 && gy < G.ny && gz >= 0 && gz < G.nz)
+        v = x[((long long)gx + (long long)G.nx * (gy + (long long)G.ny * gz)) * CIN + c];
+      halo[hv * HP + c] = v;
+    }
+    __syncthreads();
+    for (int tap = 0; tap < 27; ++tap) {
+      const int b = gpar;
+      if (used[b]) {   // the MMAs that read this buffer two taps ago must be done
+        const bool ok = mbar_wait(smem_u32(&mbar[b]), phase[b]);
+        phase[b] ^= 1u;
+        if (__syncthreads_or(!ok)) { failed = true; break; }
+      }
+      unsigned char* hi = asm_ + (size_t)b * 2 * kCvPlane;
+      unsigned char* lo = hi + kCvPlane;
+      const int dx = tap % 3, dy = (tap / 3) % 3, dz = tap / 9;
+      for (int e = tid; e < 128 * CIN; e += kCvThreads) {
+        const int a = e / CIN, k = e - a * CIN;
+        const int lx = a & 7, ly = (a >> 3) & 3, lz = a >> 5;
+        const float v = halo[((lx + dx) + kCvHX * ((ly + dy) + kCvHY * (lz + dz))) * HP + k];
+        const uint32_t h = tf32_rna(v);
+        const int o = op_offset(a, k);
+        *reinterpret_cast<uint32_t*>(hi + o) = h;
+        *reinterpret_cast<float*>(lo + o) = v - __uint_as_float(h);
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncthreads();
+      if (tid == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        const uint32_t ah = smem_u32(hi), al = smem_u32(lo);
+        const uint32_t wt = smem_u32(wsm + (size_t)tap * NP * 128);
 #pragma unroll
-          for (int c4 = 0; c4 < COP / 4; ++c4) {
-            const float4 w = w4[c4];
-            acc0[4 * c4 + 0] = fmaf(xa, w.x, acc0[4 * c4 + 0]);
-            acc0[4 * c4 + 1] = fmaf(xa, w.y, acc0[4 * c4 + 1]);
-            acc0[4 * c4 + 2] = fmaf(xa, w.z, acc0[4 * c4 + 2]);
-            acc0[4 * c4 + 3] = fmaf(xa, w.w, acc0[4 * c4 + 3]);
-            acc1[4 * c4 + 0] = fmaf(xb, w.x, acc1[4 * c4 + 0]);
-            acc1[4 * c4 + 1] = fmaf(xb, w.y, acc1[4 * c4 + 1]);
-            acc1[4 * c4 + 2] = fmaf(xb, w.z, acc1[4 * c4 + 2]);
-            acc1[4 * c4 + 3] = fmaf(xb, w.w, acc1[4 * c4 + 3]);
-          }
+        for (int s = 0; s < 4; ++s) {
+          const uint64_t dw = umma_desc_sw128(wt + s * 32);
+          umma_tf32(tmem, umma_desc_sw128(ah + s * 32), dw, idesc, (tap > 0 || s > 0) ? 1u : 0u);
+          umma_tf32(tmem, umma_desc_sw128(al + s * 32), dw, idesc, 1u);
+        }
+        umma_commit(smem_u32(&mbar[b]));
+        if (tap == 26) umma_commit(smem_u32(&mbar[2]));
+      }
+      used[b] = true;
+      gpar ^= 1;
+    }
+    if (failed) break;
+    {
+      const bool ok = mbar_wait(smem_u32(&mbar[2]), phase[2]);
+      phase[2] ^= 1u;
+      for (int bb = 0; bb < 2; ++bb)
+        if (used[bb]) {
+          mbar_wait(smem_u32(&mbar[bb]), phase[bb]);
+          phase[bb] ^= 1u;
+          used[bb] = false;
+        }
+      if (__syncthreads_or(!ok)) { failed = true; break; }
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (warp < 4) {   // warp w holds TMEM lanes 32 w .. 32 w + 31 = tile rows (voxels)
+      uint32_t r[NP];
+      const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16);
+      if constexpr (NP == 32) {
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+            "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+              "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]),
+              "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]),
+              "=r"(r[30]), "=r"(r[31])
+            : "r"(taddr));
+      } else {
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+            : "r"(taddr));
+      }
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      const int a = 32 * warp + lane;
+      const int gx = ox + (a & 7), gy = oy + ((a >> 3) & 3), gz = oz + (a >> 5);
+      if (gx < G.nx && gy < G.ny && gz < G.nz) {
+        const long long v = (long long)gx + (long long)G.nx * (gy + (long long)G.ny * gz);
+#pragma unroll
+        for (int c = 0; c < COUT; ++c) {
+          float val = __uint_as_float(r[c]) + (bias ? bias[c] : 0.f);
+          if (relu) val = fmaxf(val, 0.f);
+          if (add) val += add[v * COUT + c];
+          y[v * COUT + c] = val;
         }
       }
-  auto store = [&](const float (&a)[COP], int gz) {
-    const int gx = ox + lx, gy = oy + ly;
-    if (gx >= G.nx || gy >= G.ny || gz >= G.nz) return;
-    const long long v = (long long)gx + (long long)G.nx * (gy + (long long)G.ny * gz);
-#pragma unroll
-    for (int c = 0; c < COUT; ++c) {
-      float val = a[c];
-      if (relu) val = fmaxf(val, 0.f);
-      if (add) val += add[v * COUT + c];
-      y[v * COUT + c] = val;
     }
-  };
-  store(acc0, oz + lz);
-  store(acc1, oz + lz + 2);
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+  }
+  if (failed && tid == 0 && err) atomicExch(err, 1);
+  // nothing may still write the accumulator when it is released
+  if (tid == 0) umma_commit(smem_u32(&mbar[2]));
+  mbar_wait(smem_u32(&mbar[2]), phase[2]);
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(32u));
 }
 
-// Partial weight (and bias) gradients of one conv layer over the CTA's tiles:
-// dW[tap][ci][co] = sum_v x[v + d(tap) - 1][ci] dy[v][co], db[co] = sum_v dy[v][co].
+// ---------------------------------------------------------------------------------------
+// Weight gradient on the tensor cores: D[(tap, ci)][co] = sum_v x[v + d(tap)][ci] dy[v][co]
+// as MT = ceil(27 CIN / 128) GEMMs of M = 128 rows (tap, ci), N = COUT (padded to 16 / 32),
+// K = voxels, accumulated in tensor memory over every tile the CTA visits (MT x N columns).
+// Per 128-voxel tile the input halo and the tile's dy are staged once; dy goes to TF32 hi / lo
+// B planes (N rows x 32 voxels per K chunk), and for each (K chunk, M tile) the tap-shifted
+// input rows are written as hi / lo A planes (double-buffered) and multiplied with 3xTF32
+// (hi hi + hi lo + lo hi).  At the end each CTA writes its partial sums (and the bias
+// gradient, summed in FP32 from the staged dy); a fixed-order reduction adds the CTAs.
+// ---------------------------------------------------------------------------------------
 template <int CIN, int COUT>
-__global__ void __launch_bounds__(kWgThreads) conv3d_wgrad_kernel(const float* __restrict__ x,
-                                                                  const float* __restrict__ dy, float* __restrict__ part,
-                                                                  TileGeo G, long long ntiles) {
-  constexpr int CP = odd_pitch(CIN), COP = pad4(COUT);
-  constexpr int NP = 27 * CIN;
-  constexpr int PPT = (NP + kWgThreads - 1) / kWgThreads;
-  extern __shared__ __align__(16) float smem_f[];
-  float* s_dy = smem_f;              // [kTV][COP]
-  float* s_in = smem_f + kTV * COP;  // [kHV][CP]
-  const int t = threadIdx.x;
-  int hoff[PPT], cidx[PPT];
-#pragma unroll
-  for (int k = 0; k < PPT; ++k) {
-    const int p = t + kWgThreads * k;
-    const int tap = p < NP ? p / CIN : 0;
-    cidx[k] = p < NP ? p - tap * CIN : -1;
-    const int dx = tap % 3, dyy = (tap / 3) % 3, dz = tap / 9;
-    hoff[k] = (dz * kHY + dyy) * kHX + dx;
+struct WgLayout {
+  static constexpr int NP = cv_np(COUT);
+  static constexpr int HP = CIN | 1;
+  static constexpr int MT = (27 * CIN + 127) / 128;
+  static constexpr int TCOLS = MT * NP <= 32 ? 32 : MT * NP <= 64 ? 64 : MT * NP <= 128 ? 128 : 256;
+  static constexpr size_t off_hdr = 0;
+  static constexpr size_t off_b = 1024;                              // 4 K chunks x (hi, lo) x NP x 128 B
+  static constexpr size_t off_a = off_b + (size_t)8 * NP * 128;       // 2 buffers x (hi, lo)
+  static constexpr size_t off_halo = off_a + (size_t)4 * kCvPlane;
+  static constexpr size_t off_dy = off_halo + sizeof(float) * (size_t)kCvHV * HP;
+  static constexpr size_t total = off_dy + sizeof(float) * 128 * COUT;
+};
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(kCvThreads, 1) conv3d_wgrad_tc_kernel(const float* __restrict__ x,
+                                                                        const float* __restrict__ dy,
+                                                                        float* __restrict__ part, CvGeo G, int* err) {
+  using Lay = WgLayout<CIN, COUT>;
+  constexpr int NP = Lay::NP, HP = Lay::HP, MT = Lay::MT, ROWS = 27 * CIN;
+  constexpr uint32_t idesc = umma_idesc_tf32(128, NP);
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned long long* mbar = reinterpret_cast<unsigned long long*>(smem + Lay::off_hdr);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + Lay::off_hdr + 32);
+  unsigned char* bsm = smem + Lay::off_b;
+  unsigned char* asm_ = smem + Lay::off_a;
+  float* halo = reinterpret_cast<float*>(smem + Lay::off_halo);
+  float* sdy = reinterpret_cast<float*>(smem + Lay::off_dy);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"((uint32_t)Lay::TCOLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
-  float acc[PPT][COUT];
-#pragma unroll
-  for (int k = 0; k < PPT; ++k)
-#pragma unroll
-    for (int c = 0; c < COUT; ++c) acc[k][c] = 0.f;
+  if (tid == 0) {
+    for (int b = 0; b < 3; ++b) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[b])));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  for (int i = tid; i < (int)((Lay::off_halo - Lay::off_b) / 16); i += kCvThreads)
+    reinterpret_cast<float4*>(bsm)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = *tmem_slot;
+  uint32_t phase[3] = {0u, 0u, 0u};
+  bool used[2] = {false, false};
+  bool failed = false, first = true;
+  int gpar = 0;
   float dbacc = 0.f;
-  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    int ox, oy, oz;
-    G.origin(tile, ox, oy, oz);
-    __syncthreads();
-    load_halo<CIN>(x, s_in, G, ox, oy, oz);
-    for (int i = t; i < kTV * COP; i += blockDim.x) {
-      const int lv = i / COP, c = i - lv * COP;
-      const int gx = ox + (lv & 7), gy = oy + ((lv >> 3) & 7), gz = oz + (lv >> 6);
+  for (long long tile = blockIdx.x; tile < G.ntiles && !failed; tile += gridDim.x) {
+    const int ox = (int)(tile % G.tx) * kCvTX;
+    const long long rt = tile / G.tx;
+    const int oy = (int)(rt % G.ty) * kCvTY, oz = (int)(rt / G.ty) * kCvTZ;
+    for (int i = tid; i < kCvHV * CIN; i += kCvThreads) {
+      const int hv = i / CIN, c = i - hv * CIN;
+      const int hx = hv % kCvHX, hy = (hv / kCvHX) % kCvHY, hz = hv / (kCvHX * kCvHY);
+      const int gx = ox + hx - 1, gy = oy + hy - 1, gz = oz + hz - 1;
       float v = 0.f;
-      if (c < COUT && gx < G.nx && gy < G.ny && gz < G.nz)
-        v = dy[((long long)gx + (long long)G.nx * (gy + (long long)G.ny * gz)) * COUT + c];
-      s_dy[i] = v;
+      if (gx >= 0 && gx < G.nx && gy >= 0 && gy < G.ny && gz >= 0 && gz < G.nz)
+        v = x[((long long)gx + (long long)G.nx * (gy + (long long)G.ny * gz)) * CIN + c];
+      halo[hv * HP + c] = v;
+    }
+    for (int i = tid; i < 128 * COUT; i += kCvThreads) {   // dy of the tile's voxels -> B planes (row co, column voxel)
+      const int a = i / COUT, c = i - a * COUT;
+      const int gx = ox + (a & 7), gy = oy + ((a >> 3) & 3), gz = oz + (a >> 5);
+      float v = 0.f;
+      if (gx < G.nx && gy < G.ny && gz < G.nz) v = dy[((long long)gx + (long long)G.nx * (gy + (long long)G.ny * gz)) * COUT + c];
+      sdy[i] = v;
+      const int kc = a >> 5, kv = a & 31;
+      unsigned char* bh = bsm + (size_t)kc * 2 * NP * 128;
+      const uint32_t h = tf32_rna(v);
+      const int o = op_offset(c, kv);
+      *reinterpret_cast<uint32_t*>(bh + o) = h;
+      *reinterpret_cast<float*>(bh + NP * 128 + o) = v - __uint_as_float(h);
     }
     __syncthreads();
-#pragma unroll 1
-    for (int lv = 0; lv < kTV; ++lv) {
-      const int hb = ((lv >> 6) * kHY + ((lv >> 3) & 7)) * kHX + (lv & 7);
-      float d[COP];
+    if (tid < COUT)
+      for (int a = 0; a < 128; ++a) dbacc += sdy[a * COUT + tid];
+    for (int kc = 0; kc < 4 && !failed; ++kc) {
+      for (int mt = 0; mt < MT; ++mt) {
+        const int b = gpar;
+        if (used[b]) {
+          const bool ok = mbar_wait(smem_u32(&mbar[b]), phase[b]);
+          phase[b] ^= 1u;
+          if (__syncthreads_or(!ok)) { failed = true; break; }
+        }
+        unsigned char* hi = asm_ + (size_t)b * 2 * kCvPlane;
+        unsigned char* lo = hi + kCvPlane;
+        for (int e = tid; e < 128 * 32; e += kCvThreads) {   // row r = (tap, ci), column kv = voxel 32 kc + kv
+          const int rl = e >> 5, kv = e & 31;
+          const int r = mt * 128 + rl;
+          float v = 0.f;
+          if (r < ROWS) {
+            const int tap = r / CIN, ci = r - tap * CIN;
+            const int dx = tap % 3, dyy = (tap / 3) % 3, dz = tap / 9;
+            const int a = 32 * kc + kv;
+            const int lx = a & 7, ly = (a >> 3) & 3, lz = a >> 5;
+            v = halo[((lx + dx) + kCvHX * ((ly + dyy) + kCvHY * (lz + dz))) * HP + ci];
+          }
+          const uint32_t h = tf32_rna(v);
+          const int o = op_offset(rl, kv);
+          *reinterpret_cast<uint32_t*>(hi + o) = h;
+          *reinterpret_cast<float*>(lo + o) = v - __uint_as_float(h);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+          asm volatile("tcgen05.fence::after_thread_sync;");
+          const uint32_t ah = smem_u32(hi), al = smem_u32(lo);
+          const uint32_t bh = smem_u32(bsm + (size_t)kc * 2 * NP * 128), bl = bh + NP * 128;
+          const uint32_t d = tmem + (uint32_t)(mt * NP);
 #pragma unroll
-      for (int c4 = 0; c4 < COP / 4; ++c4) {
-        const float4 w = reinterpret_cast<const float4*>(s_dy + lv * COP)[c4];
-        d[4 * c4] = w.x; d[4 * c4 + 1] = w.y; d[4 * c4 + 2] = w.z; d[4 * c4 + 3] = w.w;
+          for (int st = 0; st < 4; ++st) {
+            const uint64_t dah = umma_desc_sw128(ah + st * 32), dal = umma_desc_sw128(al + st * 32);
+            const uint64_t dbh = umma_desc_sw128(bh + st * 32), dbl = umma_desc_sw128(bl + st * 32);
+            umma_tf32(d, dah, dbh, idesc, (first && kc == 0 && st == 0) ? 0u : 1u);
+            umma_tf32(d, dah, dbl, idesc, 1u);
+            umma_tf32(d, dal, dbh, idesc, 1u);
+          }
+          umma_commit(smem_u32(&mbar[b]));
+          if (kc == 3 && mt == MT - 1) umma_commit(smem_u32(&mbar[2]));
+        }
+        used[b] = true;
+        gpar ^= 1;
       }
-#pragma unroll
-      for (int k = 0; k < PPT; ++k) {
-        if (cidx[k] < 0) continue;
-        const float xv = s_in[(hb + hoff[k]) * CP + cidx[k]];
-#pragma unroll
-        for (int c = 0; c < COUT; ++c) acc[k][c] = fmaf(xv, d[c], acc[k][c]);
-      }
-      if (t < COUT) dbacc += s_dy[lv * COP + t];
+    }
+    if (failed) break;
+    first = false;
+    {   // the next tile overwrites the B planes and the halo: this tile's MMAs must be done
+      const bool ok = mbar_wait(smem_u32(&mbar[2]), phase[2]);
+      phase[2] ^= 1u;
+      for (int bb = 0; bb < 2; ++bb)
+        if (used[bb]) {
+          mbar_wait(smem_u32(&mbar[bb]), phase[bb]);
+          phase[bb] ^= 1u;
+          used[bb] = false;
+        }
+      if (__syncthreads_or(!ok)) { failed = true; break; }
     }
   }
-  float* P = part + (long long)blockIdx.x * (NP * COUT + COUT);
+  float* P = part + (long long)blockIdx.x * (ROWS * COUT + COUT);
+  if (!failed) {
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (warp < 4) {
+      for (int mt = 0; mt < MT; ++mt) {
+        uint32_t r[NP];
+        const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(mt * NP);
+        if constexpr (NP == 32) {
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+              "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+              : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+                "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+                "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+              : "r"(taddr));
+        } else {
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+              : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                "=r"(r[15])
+              : "r"(taddr));
+        }
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        const int row = mt * 128 + 32 * warp + lane;
+        if (row < ROWS) {
 #pragma unroll
-  for (int k = 0; k < PPT; ++k) {
-    const int p = t + kWgThreads * k;
-    if (p < NP)
-#pragma unroll
-      for (int c = 0; c < COUT; ++c) P[(long long)p * COUT + c] = acc[k][c];
+          for (int c = 0; c < COUT; ++c) P[(long long)row * COUT + c] = first ? 0.f : __uint_as_float(r[c]);
+        }
+      }
+    }
+    if (tid < COUT) P[ROWS * COUT + tid] = dbacc;
   }
-  if (t < COUT) P[NP * COUT + t] = dbacc;
+  if (failed && tid == 0 && err) atomicExch(err, 1);
+  if (tid == 0) umma_commit(smem_u32(&mbar[2]));
+  mbar_wait(smem_u32(&mbar[2]), phase[2]);
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)Lay::TCOLS));
 }
 
 // out[i] = sum over `nb` partial blocks (fixed order), i < n
@@ -368,60 +573,54 @@ bool conv_shape_ok(int cin, int cout) {
 }
 
 template <int CIN, int COUT>
-size_t conv_smem() {
-  return sizeof(float) * (27 * CIN * pad4(COUT) + kHV * odd_pitch(CIN));
-}
-template <int CIN, int COUT>
-size_t wgrad_smem() {
-  return sizeof(float) * (kTV * pad4(COUT) + kHV * odd_pitch(CIN));
-}
-
-TileGeo tile_geo(const int* dims) {
-  TileGeo G;
-  G.nx = dims[0]; G.ny = dims[1]; G.nz = dims[2];
-  G.tx = (G.nx + kTX - 1) / kTX;
-  G.ty = (G.ny + kTY - 1) / kTY;
-  return G;
-}
-long long tile_count(const int* dims) {
-  return (long long)((dims[0] + kTX - 1) / kTX) * ((dims[1] + kTY - 1) / kTY) * ((dims[2] + kTZ - 1) / kTZ);
-}
-
-template <int CIN, int COUT>
 int conv_inst(const float* x, const uint16_t* w, const float* b, const float* add, float* y, const int* dims, int relu,
-              cudaStream_t s) {
-  const size_t smem = conv_smem<CIN, COUT>();
-  auto k = conv3d_kernel<CIN, COUT>;
+              int* err, cudaStream_t s) {
+  const size_t smem = CvLayout<CIN, COUT>::total;
+  static_assert(CvLayout<CIN, COUT>::total <= 227 * 1024, "conv operands exceed shared memory");
+  auto k = conv3d_tc_kernel<CIN, COUT>;
   LLR_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const long long nt = tile_count(dims);
+  int dev = 0, nsm = 0;
+  LLR_CUDA_TRY(cudaGetDevice(&dev));
+  LLR_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  CvGeo G;
+  G.nx = dims[0]; G.ny = dims[1]; G.nz = dims[2];
+  G.tx = (G.nx + kCvTX - 1) / kCvTX;
+  G.ty = (G.ny + kCvTY - 1) / kCvTY;
+  G.ntiles = (long long)G.tx * G.ty * ((G.nz + kCvTZ - 1) / kCvTZ);
+  const long long grid = std::min<long long>(G.ntiles, nsm);
   note_launch();
-  k<<<(unsigned)nt, kConvThreads, smem, s>>>(x, w, b, add, y, tile_geo(dims), relu);
+  k<<<(unsigned)grid, kCvThreads, smem, s>>>(x, w, b, add, y, G, relu, err);
   LLR_CUDA_TRY(cudaGetLastError());
   return LLR_OK;
 }
 
 int conv(int cin, int cout, const float* x, const uint16_t* w, const float* b, const float* add, float* y,
-         const int* dims, int relu, cudaStream_t s) {
-  if (cin == 14 && cout == 32) return conv_inst<14, 32>(x, w, b, add, y, dims, relu, s);
-  if (cin == 32 && cout == 32) return conv_inst<32, 32>(x, w, b, add, y, dims, relu, s);
-  if (cin == 32 && cout == 14) return conv_inst<32, 14>(x, w, b, add, y, dims, relu, s);
+         const int* dims, int relu, int* err, cudaStream_t s) {
+  if (cin == 14 && cout == 32) return conv_inst<14, 32>(x, w, b, add, y, dims, relu, err, s);
+  if (cin == 32 && cout == 32) return conv_inst<32, 32>(x, w, b, add, y, dims, relu, err, s);
+  if (cin == 32 && cout == 14) return conv_inst<32, 14>(x, w, b, add, y, dims, relu, err, s);
   return set_error(LLR_ERR_UNSUPPORTED, "conv3d %d -> %d channels is not built", cin, cout);
 }
 
 template <int CIN, int COUT>
-int wgrad_inst(const float* x, const float* dy, float* part, long long part_cap, float* out, const int* dims,
+int wgrad_inst(const float* x, const float* dy, float* part, long long part_cap, float* out, const int* dims, int* err,
                cudaStream_t s) {
-  const size_t smem = wgrad_smem<CIN, COUT>();
-  auto k = conv3d_wgrad_kernel<CIN, COUT>;
+  const size_t smem = WgLayout<CIN, COUT>::total;
+  static_assert(WgLayout<CIN, COUT>::total <= 227 * 1024, "wgrad operands exceed shared memory");
+  auto k = conv3d_wgrad_tc_kernel<CIN, COUT>;
   LLR_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int dev = 0, nsm = 0;
   LLR_CUDA_TRY(cudaGetDevice(&dev));
   LLR_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  const long long nt = tile_count(dims);
+  CvGeo G;
+  G.nx = dims[0]; G.ny = dims[1]; G.nz = dims[2];
+  G.tx = (G.nx + kCvTX - 1) / kCvTX;
+  G.ty = (G.ny + kCvTY - 1) / kCvTY;
+  G.ntiles = (long long)G.tx * G.ty * ((G.nz + kCvTZ - 1) / kCvTZ);
   const long long per = 27LL * CIN * COUT + COUT;
-  const int grid = (int)std::max<long long>(1, std::min<long long>(std::min<long long>(nt, 2LL * nsm), part_cap / per));
+  const int grid = (int)std::max<long long>(1, std::min<long long>(std::min<long long>(G.ntiles, nsm), part_cap / per));
   note_launch();
-  k<<<grid, kWgThreads, smem, s>>>(x, dy, part, tile_geo(dims), nt);
+  k<<<grid, kCvThreads, smem, s>>>(x, dy, part, G, err);
   LLR_CUDA_TRY(cudaGetLastError());
   note_launch();
   reduce_partials_kernel<<<grid_1d(per), 256, 0, s>>>(part, grid, per, out);
@@ -430,10 +629,10 @@ int wgrad_inst(const float* x, const float* dy, float* part, long long part_cap,
 }
 
 int wgrad(int cin, int cout, const float* x, const float* dy, float* part, long long cap, float* out, const int* dims,
-          cudaStream_t s) {
-  if (cin == 14 && cout == 32) return wgrad_inst<14, 32>(x, dy, part, cap, out, dims, s);
-  if (cin == 32 && cout == 32) return wgrad_inst<32, 32>(x, dy, part, cap, out, dims, s);
-  if (cin == 32 && cout == 14) return wgrad_inst<32, 14>(x, dy, part, cap, out, dims, s);
+          int* err, cudaStream_t s) {
+  if (cin == 14 && cout == 32) return wgrad_inst<14, 32>(x, dy, part, cap, out, dims, err, s);
+  if (cin == 32 && cout == 32) return wgrad_inst<32, 32>(x, dy, part, cap, out, dims, err, s);
+  if (cin == 32 && cout == 14) return wgrad_inst<32, 14>(x, dy, part, cap, out, dims, err, s);
   return set_error(LLR_ERR_UNSUPPORTED, "conv3d %d -> %d channels is not built", cin, cout);
 }
 
@@ -482,7 +681,7 @@ int forward(llr_cnn* n, const float* in, float* out, const int* dims, cudaStream
     const bool last = l + 1 == n->n_layers;
     float* y = last ? out : n->act[l + 1];
     LLR_TRY(conv(n->cin[l], n->cout[l], n->act[l], n->d_wb + wtab_off(n, l), n->d_master + n->b_off[l],
-                 last ? in : nullptr, y, dims, last ? 0 : 1, s));
+                 last ? in : nullptr, y, dims, last ? 0 : 1, n->d_err, s));
   }
   return LLR_OK;
 }
@@ -539,6 +738,8 @@ int llr_cnn_create(int32_t n_layers, const int32_t* channels, int32_t device, ui
   for (int l = 0; l < n_layers; ++l) maxw = std::max(maxw, 27LL * channels[l] * channels[l + 1] + channels[l + 1]);
   n->part_cap = maxw * 2 * 148;
   if (e == cudaSuccess) e = cudaMalloc((void**)&n->d_part, sizeof(float) * n->part_cap);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&n->d_err, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(n->d_err, 0, sizeof(int));
   if (e != cudaSuccess) return fail(cuda_error(e, "cudaMalloc", __FILE__, __LINE__));
   e = cudaMemset(n->d_master, 0, sizeof(float) * off);
   if (e == cudaSuccess) e = cudaMemset(n->d_m, 0, sizeof(float) * off);
@@ -570,7 +771,8 @@ int llr_cnn_destroy(llr_cnn* n) {
   cudaSetDevice(n->device);
   for (int l = 1; l < (int)n->act.size(); ++l) if (n->act[l]) cudaFree(n->act[l]);
   for (void* p : {(void*)n->d_master, (void*)n->d_grad, (void*)n->d_m, (void*)n->d_v, (void*)n->d_wb, (void*)n->d_wt,
-                  (void*)n->d_g0, (void*)n->d_g1, (void*)n->d_out, (void*)n->d_part, (void*)n->d_loss})
+                  (void*)n->d_g0, (void*)n->d_g1, (void*)n->d_out, (void*)n->d_part, (void*)n->d_loss,
+                  (void*)n->d_err})
     if (p) cudaFree(p);
   delete n;
   return LLR_OK;
@@ -631,10 +833,11 @@ int llr_cnn_loss_grad_dev(llr_cnn* n, const float* d_in, const float* d_target, 
   float* g = n->d_g0;
   float* gn = n->d_g1;
   for (int l = n->n_layers - 1; l >= 0; --l) {
-    LLR_TRY(wgrad(n->cin[l], n->cout[l], n->act[l], g, n->d_part, n->part_cap, n->d_grad + n->w_off[l], dims, s));
+    LLR_TRY(wgrad(n->cin[l], n->cout[l], n->act[l], g, n->d_part, n->part_cap, n->d_grad + n->w_off[l], dims,
+                  n->d_err, s));
     if (l == 0) break;
     // dL/d act[l] = conv(g, W') masked by the ReLU that produced act[l]
-    LLR_TRY(conv(n->cout[l], n->cin[l], g, n->d_wt + wtab_off(n, l), nullptr, nullptr, gn, dims, 0, s));
+    LLR_TRY(conv(n->cout[l], n->cin[l], g, n->d_wt + wtab_off(n, l), nullptr, nullptr, gn, dims, 0, n->d_err, s));
     const long long na = vox * n->cin[l];
     note_launch();
     relu_mask_kernel<<<grid_1d(na), 256, 0, s>>>(gn, n->act[l], na);
@@ -648,6 +851,9 @@ int llr_cnn_loss_grad_dev(llr_cnn* n, const float* d_in, const float* d_target, 
     double t = 0.0;
     for (double v : h) t += v;
     *loss = t / (double)nout;
+    int herr = 0;
+    LLR_CUDA_TRY(cudaMemcpy(&herr, n->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (herr) return set_error(LLR_ERR_CUDA, "a tensor-core wait in a conv3d kernel timed out");
   }
   return LLR_OK;
 }

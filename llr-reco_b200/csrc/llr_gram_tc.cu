@@ -18,6 +18,7 @@
 #include <algorithm>
 
 #include "llr_prox_common.cuh"
+#include "llr_umma.cuh"
 
 namespace llr {
 
@@ -28,8 +29,6 @@ constexpr int kTcThreads = 32 * kTcWarps;
 constexpr int kKC = 32;                    // rows (K) per staged chunk
 constexpr int kQT = (64 + kTcWarps - 1) / kTcWarps;   // volumes per warp per chunk (kTcWarps x kQT >= n)
 constexpr int kOpBytes = 128 * kKC * 4;    // one operand plane (hi or lo) of one chunk
-constexpr unsigned long long kWaitLimit = 1ull << 22;   // bounded spin: ~seconds, never forever
-
 // Row table of one block: planar offset of every row and either the row's phase (uniform
 // over the volumes) or its coordinates (per-volume phase).  The kernel keeps kRowBufs tables:
 // the one of the block being converted and those of the blocks whose chunks are prefetched.
@@ -52,59 +51,8 @@ struct TcHdr {
   int pad;
 };
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-// K-major UMMA shared-memory descriptor (sm_100 version 1) with the 128-byte swizzle: rows of
-// 128 B (32 TF32 along K), 8-row atoms of 1 KB (SBO = 1 KB), the 16-byte chunk index XORed with
-// the row index inside the atom.  Stepping K by 8 TF32 moves the start address by 32 B.
-__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
-  uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
-  d |= (uint64_t)1 << 16;                          // LBO: unused for swizzled K-major
-  d |= (uint64_t)(1024u >> 4) << 32;               // SBO: next 8-row atom
-  d |= (uint64_t)1 << 46;
-  d |= (uint64_t)2 << 61;                          // SWIZZLE_128B
-  return d;
-}
-
 // Instruction descriptor: TF32 x TF32 -> F32, both K-major, M = 128, N = 128.
-constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
-
-__device__ __forceinline__ void umma_tf32(uint32_t d, uint64_t a, uint64_t b, uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
-      "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate));
-}
-
-__device__ __forceinline__ void umma_commit(uint32_t mbar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try(uint32_t mbar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
-      "selp.b32 %0, 1, 0, P1;\n\t}" : "=r"(ok) : "r"(mbar), "r"(parity) : "memory");
-  return ok != 0;
-}
-
-// Bounded wait; returns false when the limit runs out.
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
-  for (unsigned long long i = 0; i < kWaitLimit; ++i)
-    if (mbar_try(mbar, parity)) return true;
-  return false;
-}
-
-// TF32 part of x rounded to nearest (ties away from zero) on the 10-bit mantissa: add half a
-// TF32 unit to the magnitude bits and clear the 13 low bits.  Finite inputs only (the iterate).
-__device__ __forceinline__ uint32_t tf32_rna(float x) {
-  return (__float_as_uint(x) + 0x1000u) & 0xFFFFE000u;
-}
-
-// Byte offset of element (mn, k) of one operand plane (k < 32) in the 128-byte swizzled layout.
-__device__ __forceinline__ int op_offset(int mn, int k) {
-  return (mn >> 3) * 1024 + (mn & 7) * 128 + ((((k >> 2) ^ mn) & 7) << 4) + ((k & 3) << 2);
-}
+constexpr uint32_t kIdesc = umma_idesc_tf32(128, 128);
 
 template <int NPMAX>
 __global__ void __launch_bounds__(kTcThreads, 3) llr_gram_tc_kernel(BlockSource src, ProxOp op, TcLayout L) {
@@ -232,9 +180,9 @@ __global__ void __launch_bounds__(kTcThreads, 3) llr_gram_tc_kernel(BlockSource 
       for (int s = 0; s < kKC / 8; ++s) {
         const uint64_t dh = umma_desc_sw128(ah + s * 32);
         const uint64_t dl = umma_desc_sw128(al + s * 32);
-        umma_tf32(tmem, dh, dh, (c > 0 || s > 0) ? 1u : 0u);
-        umma_tf32(tmem, dh, dl, 1u);
-        umma_tf32(tmem, dl, dh, 1u);
+        umma_tf32(tmem, dh, dh, kIdesc, (c > 0 || s > 0) ? 1u : 0u);
+        umma_tf32(tmem, dh, dl, kIdesc, 1u);
+        umma_tf32(tmem, dl, dh, kIdesc, 1u);
       }
       umma_commit(smem_u32(&hdr->mbar[b]));
       if (c == nchunks - 1) umma_commit(smem_u32(&hdr->mbar[2]));
