@@ -277,6 +277,8 @@ def workload_label(name: str, c: dict, nq: int) -> str:
         extra = (f", rank-{c['srank']} temporal subspace (LLR on coefficients), "
                  f"{c['wavelet_levels']}-level db{c['wavelet_moments']} wavelet shrink alpha {c['wavelet_alpha']:g} "
                  f"on the {where}")
+    if "stride" in c:
+        extra += f", overlapping blocks at stride {c['stride'][0]} (each voxel the mean of its block outputs)"
     return (f"{name}: {v[0]}x{v[1]}x{v[2]} complex64 x {nq} volumes, {b[0]}^3 LLR blocks (Casorati "
             f"{b[0] * b[1] * b[2]}x{n}){extra}, {c['accel']:g}x VD line sampling, soft threshold 0.02 sigma_max, "
             f"FP32, one proximal-gradient iteration per step")
@@ -297,7 +299,7 @@ def run_b200(args, dist: Dist) -> None:
     E = nx * ny * nz * nq
     params = ReconParams(vol_size=(nx, ny, nz), nq=nq, block_size=c["block"], prox_mode=llr_b200.LLR_PROX_SOFT_THRESH,
                          lam=0.0, seed=args.seed, device=dev, gram_mode=args.gram_mode,
-                         eig_solver=args.eig_solver, fft_mode=args.fft_mode)
+                         eig_solver=args.eig_solver, fft_mode=args.fft_mode, block_stride=c.get("stride"))
     if "srank" in c:   # subspace + wavelet configuration: subspace built on the GPU from the b-table
         from llr_b200.phantom import dti_subspace_gpu
         params.subspace_rank = c["srank"]

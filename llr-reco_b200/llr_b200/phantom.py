@@ -164,6 +164,11 @@ CONFIGS = {
     "c2_small": dict(vol=(96, 96, 48), shells=[(0, 7), (3000, 54)], accel=8.0, block=(6, 6, 6), n_iter=100),
     "c3": dict(vol=(256, 256, 256), shells=[(0, 1), (1000, 30), (2000, 30)], accel=10.0, block=(8, 8, 8),
                n_iter=80, srank=7, wavelet_alpha=0.005, wavelet_moments=4, wavelet_levels=3, wavelet_space=1),
+    "c5": dict(vol=(256, 256, 256), shells=[(0, 6), (1000, 34), (2000, 33), (3000, 33)], accel=12.0,
+               block=(8, 8, 8), stride=(4, 4, 4), n_iter=80),
+    # config-5 geometry class at 1/8 of the volume (1.78 GB per copy): measurement case
+    "c5_small": dict(vol=(128, 128, 128), shells=[(0, 6), (1000, 34), (2000, 33), (3000, 33)], accel=12.0,
+                     block=(8, 8, 8), stride=(4, 4, 4), n_iter=80),
 }
 
 
