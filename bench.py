@@ -156,8 +156,8 @@ def write_traffic(args) -> None:
     ``--traffic-scale`` (units processed at the target size / units in the capture) and write
     profiles/<--traffic-name>_<--config>.json."""
     import csv
-    with open(args.ncu_traffic) as f:
-        rows = [r for r in csv.reader(f) if r]
+    with open(args.ncu_traffic) as f:   # ncu's own log lines (==PROF==, ==WARNING==) precede the table
+        rows = [r for r in csv.reader([ln for ln in f.read().splitlines() if ln.startswith('"')]) if r]
     head = rows[0]
     units = rows[1]
     ik, ir, iw = head.index("Kernel Name"), head.index("dram__bytes_read.sum"), head.index("dram__bytes_write.sum")

@@ -739,6 +739,7 @@ int llr_iterate_profiled(llr_ctx* c, int32_t n, double* stage_ms, double* total_
     cudaError_t e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) st = cuda_error(e, "cudaStreamSynchronize", __FILE__, __LINE__);
   }
+  if (st == LLR_OK) st = llr::check_device_error(c);
   if (st == LLR_OK) {
     double acc[5] = {0, 0, 0, 0, 0};
     for (int it = 0; it < n; ++it)
@@ -774,6 +775,7 @@ int llr_iterate_timed(llr_ctx* c, int32_t n, double* total_ms) {
     if (e == cudaSuccess) e = cudaEventSynchronize(b);
     if (e != cudaSuccess) st = cuda_error(e, "cudaEventSynchronize", __FILE__, __LINE__);
   }
+  if (st == LLR_OK) st = llr::check_device_error(c);
   if (st == LLR_OK) {
     float ms = 0.f;
     cudaEventElapsedTime(&ms, a, b);
