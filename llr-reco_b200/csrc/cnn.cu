@@ -88,7 +88,8 @@ __host__ __device__ constexpr int cv_np(int cout) { return cout <= 16 ? 16 : 32;
 template <int CIN, int COUT>
 struct CvLayout {
   static constexpr int NP = cv_np(COUT);
-  static constexpr int HP = CIN | 1;                               // halo channel pitch (odd)
+  static constexpr int HP = (CIN + 3) & ~3;                        // halo channel pitch: 16-byte rows
+  static constexpr int NCH = HP / 4;                               // 16-byte channel chunks per voxel
   static constexpr size_t off_hdr = 0;                             // 3 mbarriers + TMEM address
   static constexpr size_t off_w = 1024;                            // 27 tap blocks of NP x 128 B
   static constexpr size_t off_a = off_w + (size_t)27 * NP * 128;   // 2 buffers x (hi, lo)
@@ -108,7 +109,9 @@ __global__ void __launch_bounds__(kCvThreads, 1) conv3d_tc_kernel(const float* _
                                                                   const float* __restrict__ add, float* __restrict__ y,
                                                                   CvGeo G, int relu, int* err) {
   using Lay = CvLayout<CIN, COUT>;
-  constexpr int NP = Lay::NP, HP = Lay::HP;
+  constexpr int NP = Lay::NP, HP = Lay::HP, NCH = Lay::NCH;
+  constexpr int ITEMS = 128 * NCH / kCvThreads;                    // 16-byte chunks per thread per tap
+  static_assert(128 * NCH % kCvThreads == 0, "chunk count must divide over the threads");
   constexpr uint32_t idesc = umma_idesc_tf32(128, NP);
   extern __shared__ __align__(1024) unsigned char smem[];
   unsigned long long* mbar = reinterpret_cast<unsigned long long*>(smem + Lay::off_hdr);
@@ -142,19 +145,30 @@ __global__ void __launch_bounds__(kCvThreads, 1) conv3d_tc_kernel(const float* _
   bool used[2] = {false, false};
   bool failed = false;
   int gpar = 0;
+  // this thread's operand chunks: row a (tile voxel) and 4-channel chunk c, as halo index and
+  // swizzled plane offset (the same for every tap and tile)
+  int hb[ITEMS], po[ITEMS];
+#pragma unroll
+  for (int j = 0; j < ITEMS; ++j) {
+    const int e = tid + j * kCvThreads;
+    const int a = e / NCH, c = e - a * NCH;
+    const int lx = a & 7, ly = (a >> 3) & 3, lz = a >> 5;
+    hb[j] = (lx + kCvHX * (ly + kCvHY * lz)) * HP + 4 * c;
+    po[j] = (a >> 3) * 1024 + (a & 7) * 128 + (((c ^ a) & 7) << 4);
+  }
 
   for (long long tile = blockIdx.x; tile < G.ntiles && !failed; tile += gridDim.x) {
     const int ox = (int)(tile % G.tx) * kCvTX;
     const long long rt = tile / G.tx;
     const int oy = (int)(rt % G.ty) * kCvTY, oz = (int)(rt / G.ty) * kCvTZ;
-    for (int i = tid; i < kCvHV * CIN; i += kCvThreads) {
-      const int hv = i / CIN, c = i - hv * CIN;
+    for (int i = tid; i < kCvHV * HP; i += kCvThreads) {   // channels CIN..HP-1 are zero padding
+      const int hv = i / HP, c = i - hv * HP;
       const int hx = hv % kCvHX, hy = (hv / kCvHX) % kCvHY, hz = hv / (kCvHX * kCvHY);
       const int gx = ox + hx - 1, gy = oy + hy - 1, gz = oz + hz - 1;
       float v = 0.f;
-      if (gx >= 0 && gx < G.nx && gy >= 0 && gy < G.ny && gz >= 0 && gz < G.nz)
+      if (c < CIN && gx >= 0 && gx < G.nx && gy >= 0 && gy < G.ny && gz >= 0 && gz < G.nz)
         v = x[((long long)gx + (long long)G.nx * (gy + (long long)G.ny * gz)) * CIN + c];
-      halo[hv * HP + c] = v;
+      halo[i] = v;
     }
     __syncthreads();
     for (int tap = 0; tap < 27; ++tap) {
@@ -167,14 +181,16 @@ __global__ void __launch_bounds__(kCvThreads, 1) conv3d_tc_kernel(const float* _
       unsigned char* hi = asm_ + (size_t)b * 2 * kCvPlane;
       unsigned char* lo = hi + kCvPlane;
       const int dx = tap % 3, dy = (tap / 3) % 3, dz = tap / 9;
-      for (int e = tid; e < 128 * CIN; e += kCvThreads) {
-        const int a = e / CIN, k = e - a * CIN;
-        const int lx = a & 7, ly = (a >> 3) & 3, lz = a >> 5;
-        const float v = halo[((lx + dx) + kCvHX * ((ly + dy) + kCvHY * (lz + dz))) * HP + k];
-        const uint32_t h = tf32_rna(v);
-        const int o = op_offset(a, k);
-        *reinterpret_cast<uint32_t*>(hi + o) = h;
-        *reinterpret_cast<float*>(lo + o) = v - __uint_as_float(h);
+      const int toff = (dx + kCvHX * (dy + kCvHY * dz)) * HP;
+#pragma unroll
+      for (int j = 0; j < ITEMS; ++j) {
+        const float4 v = *reinterpret_cast<const float4*>(halo + hb[j] + toff);
+        uint4 h;
+        h.x = tf32_rna(v.x); h.y = tf32_rna(v.y); h.z = tf32_rna(v.z); h.w = tf32_rna(v.w);
+        const float4 l = make_float4(v.x - __uint_as_float(h.x), v.y - __uint_as_float(h.y), v.z - __uint_as_float(h.z),
+                                     v.w - __uint_as_float(h.w));
+        *reinterpret_cast<uint4*>(hi + po[j]) = h;
+        *reinterpret_cast<float4*>(lo + po[j]) = l;
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncthreads();
