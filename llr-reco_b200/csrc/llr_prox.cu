@@ -266,6 +266,7 @@ __global__ void __launch_bounds__(kLlrThreads) llr_subspace_coef_kernel(BlockSou
       for (int k = 0; k < kSubMax; ++k) z[k] = make_float2(0.f, 0.f);
       int ix = 0, iy = 0, iz = 0;
       block_row_coord(src, blk, sh, r, ix, iy, iz);
+#pragma unroll 4
       for (int q = 0; q < nq; ++q) {
         float2 v = src.data[planar_index(src.g, ix, iy, iz, q)];
         v = cscale(cmul_bc(v, phase_at(src.ph, src.g, q, ix, iy, iz)), src.load_scale);
@@ -305,6 +306,7 @@ __global__ void __launch_bounds__(256) subspace_expand_kernel(const float2* __re
     const int iy = (int)(v % g.ny);
     const long long r = v / g.ny;
     const int iz = (int)(r % g.nz), ix = (int)(r / g.nz);
+#pragma unroll 4
     for (int q = 0; q < g.nq; ++q) {
       float2 a = make_float2(0.f, 0.f);
 #pragma unroll

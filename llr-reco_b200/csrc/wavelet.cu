@@ -256,9 +256,10 @@ __global__ void __launch_bounds__(kWaveThreads) wave_synthesis_kernel(View in, V
       const int xb = xy >> 1, yb = xy & 1;
       float2 a = make_float2(0.f, 0.f);
 #pragma unroll
-      for (int j = 0; j < F; ++j) {
+      for (int jj = 0; jj < F / 2; ++jj) {   // taps with F - 2 + s - j even: j = (s & 1) + 2 jj
+        const int j = (s & 1) + 2 * jj;
         const int idx = F - 2 + s - j;
-        if ((idx & 1) == 0 && idx >= 0 && idx < 2 * cz) {
+        if (idx >= 0 && idx < 2 * cz) {
           const int lz = idx / 2 - hz0;
           const float2 cl = co[(((xb * 2 + 0) * 2 + yb) * HY + lz) * HY + ly];
           const float2 chh = co[(((xb * 2 + 1) * 2 + yb) * HY + lz) * HY + ly];
@@ -280,9 +281,10 @@ __global__ void __launch_bounds__(kWaveThreads) wave_synthesis_kernel(View in, V
       for (int xb = 0; xb < 2; ++xb) {
         float2 a = make_float2(0.f, 0.f);
 #pragma unroll
-        for (int j = 0; j < F; ++j) {
+        for (int jj = 0; jj < F / 2; ++jj) {
+          const int j = (s & 1) + 2 * jj;
           const int idx = F - 2 + s - j;
-          if ((idx & 1) == 0 && idx >= 0 && idx < 2 * cy) {
+          if (idx >= 0 && idx < 2 * cy) {
             const int ly = idx / 2 - hy0;
             const float2 cl = zs[((xb * 2 + 0) * kWS + sz) * HY + ly];
             const float2 chh = zs[((xb * 2 + 1) * kWS + sz) * HY + ly];
@@ -304,9 +306,10 @@ __global__ void __launch_bounds__(kWaveThreads) wave_synthesis_kernel(View in, V
         const int iy = sy0 + sy, iz = sz0 + sz;
         float2 a = make_float2(0.f, 0.f);
 #pragma unroll
-        for (int j = 0; j < F; ++j) {
+        for (int jj = 0; jj < F / 2; ++jj) {
+          const int j = (s & 1) + 2 * jj;
           const int idx = F - 2 + s - j;
-          if ((idx & 1) == 0 && idx >= 0 && idx < 2 * cx) {
+          if (idx >= 0 && idx < 2 * cx) {
             const int hh = idx / 2;
             const float2 cl = ring[(((hh % R) * 2 + 0) * SPT + q) * kWaveThreads + tid];
             const float2 chh = ring[(((hh % R) * 2 + 1) * SPT + q) * kWaveThreads + tid];

@@ -241,7 +241,8 @@ def test_state_errors(gpu):
 
 
 def test_unsupported_casorati_is_reported(gpu):
-    p = ReconParams(vol_size=(64, 64, 64), nq=70, block_size=(8, 8, 8), rank=2)
+    """More than 128 Casorati columns is outside every prox kernel."""
+    p = ReconParams(vol_size=(64, 64, 64), nq=130, block_size=(8, 8, 8), rank=2)
     with pytest.raises(llr_b200.LlrError) as e:
         ReconContext(p)
     assert e.value.status == L.LLR_ERR_UNSUPPORTED
