@@ -191,8 +191,8 @@ __device__ float block_sum(float v, float* red) {
 // is one barrier for the rotation angles plus one for the update.
 // ---------------------------------------------------------------------------------------
 template <int NPMAX>
-__device__ void jacobi(float2* A, float2* V, int n, float4* rot, int2* pairs, Misc* misc, int max_sweeps) {
-  constexpr int lda = NPMAX + 1;
+__device__ void jacobi(float2* A, float2* V, int n, float4* rot, int2* pairs, Misc* misc, int max_sweeps,
+                       int lda = NPMAX + 1) {
   const int tid = threadIdx.x;
   const int n2 = (n + 1) & ~1;
   const int half = n2 >> 1;
@@ -340,8 +340,7 @@ __device__ void form_W(float2* A, const float2* V, int lda, int n, const float* 
 // C <- C W in place (row blocks processed in rounds; rows of one round depend only on
 // themselves, so each round writes back after one barrier).
 template <int NPMAX, int TG>
-__device__ void apply_W(float2* Cs, int ldc, int m, int n, const float2* W) {
-  constexpr int lda = NPMAX + 1;
+__device__ void apply_W(float2* Cs, int ldc, int m, int n, const float2* W, int lda = NPMAX + 1) {
   constexpr int RT = 4;
   const int nt = (n + TG - 1) / TG;               // column tiles (interleaved columns)
   const int row_tiles_per_round = max(1, (int)blockDim.x / nt);

@@ -1113,9 +1113,13 @@ constexpr int kWideRows = 32;
 
 struct WideLayout {
   TrdLayout t;     // rc / ldch / ksplit / np and the row-table offsets for gram_block
-  size_t off_rot, off_pair, off_ev, off_g, off_act, off_A, total;
+  int lda;         // leading dimension of A (and V) = n + 1
+  int v_smem;      // 1: eigenvectors in shared memory (off_V); 0: in the per-CTA global scratch
+  size_t off_rot, off_pair, off_ev, off_g, off_act, off_A, off_V, total;
 };
 
+// The eigenvectors stay in shared memory when A and V both fit beside the row tables and the
+// row chunk (n <= 108 for 512-row blocks); wider matrices keep them in the global scratch.
 inline WideLayout make_wide_layout(int m, int n) {
   WideLayout W;
   TrdLayout& L = W.t;
@@ -1124,6 +1128,8 @@ inline WideLayout make_wide_layout(int m, int n) {
   L.ksplit = 1;
   L.rc = std::min(kWideRows, m);
   L.ldch = (L.rc & 1) ? L.rc : L.rc + 1;
+  const int np2 = (n + 1) & ~1;   // Jacobi pairs up an even count: an odd n gets one zero row / column
+  W.lda = np2 + 1;
   size_t off = 256;   // Misc
   W.off_rot = off; off = align16(off + sizeof(float4) * (kProxMaxN / 2));
   W.off_pair = off; off = align16(off + sizeof(int2) * (kProxMaxN / 2));
@@ -1132,14 +1138,19 @@ inline WideLayout make_wide_layout(int m, int n) {
   W.off_act = off; off = align16(off + sizeof(int) * kProxMaxN);
   L.off_row = off; off = align16(off + sizeof(RowTab) * (size_t)m);
   L.off_rowph = off; off = align16(off + sizeof(float2) * (size_t)m);
-  W.off_A = off; off = align16(off + sizeof(float2) * kProxMaxN * (kProxMaxN + 1));
+  W.off_A = off; off = align16(off + sizeof(float2) * (size_t)np2 * W.lda);
   L.off_C = off; off = align16(off + sizeof(float2) * (size_t)n * L.ldch);
+  const size_t vbytes = sizeof(float2) * (size_t)np2 * W.lda;
+  W.v_smem = off + vbytes <= 227 * 1024 ? 1 : 0;
+  W.off_V = off;
+  if (W.v_smem) off = align16(off + vbytes);
   L.total = W.total = off;
   return W;
 }
 
 __global__ void __launch_bounds__(kLlrThreads, 1) llr_prox_wide_kernel(BlockSource src, ProxOp op, WideLayout W) {
-  constexpr int NP = kProxMaxN, lda = NP + 1;
+  constexpr int NP = kProxMaxN;
+  const int lda = W.lda;
   extern __shared__ __align__(16) unsigned char smem[];
   Misc* misc = reinterpret_cast<Misc*>(smem);
   float4* rot = reinterpret_cast<float4*>(smem + W.off_rot);
@@ -1151,7 +1162,7 @@ __global__ void __launch_bounds__(kLlrThreads, 1) llr_prox_wide_kernel(BlockSour
   float2* rowph = reinterpret_cast<float2*>(smem + W.t.off_rowph);
   float2* A = reinterpret_cast<float2*>(smem + W.off_A);
   float2* Cch = reinterpret_cast<float2*>(smem + W.t.off_C);
-  float2* V = op.vwide + (long long)blockIdx.x * wide_v_stride();
+  float2* V = W.v_smem ? reinterpret_cast<float2*>(smem + W.off_V) : op.vwide + (long long)blockIdx.x * wide_v_stride();
   const int m = op.m, n = op.n, tid = threadIdx.x;
   const long long qstride = src.kind == 1 ? src.g.V : (long long)m;
   if (tid == 0) block_shift(src, misc->shift);
@@ -1161,10 +1172,10 @@ __global__ void __launch_bounds__(kLlrThreads, 1) llr_prox_wide_kernel(BlockSour
   for (long long i = blockIdx.x; i < count; i += gridDim.x) {
     const long long blk = src.blk_list ? (long long)src.blk_list[i] : i;
     const long long base = src.kind == 1 ? 0 : blk * (long long)m * n;
-    for (int k = tid; k < NP * lda; k += blockDim.x) A[k] = make_float2(0.f, 0.f);
+    for (int k = tid; k < ((n + 1) & ~1) * lda; k += blockDim.x) A[k] = make_float2(0.f, 0.f);
     gram_block<NP, kWideTG>(src, W.t, m, n, blk, base, qstride, sh, rows, rowph, Cch,
                             [&](int a, int b, float2 v) { A[a * lda + b] = v; });
-    jacobi<NP>(A, V, n, rot, pairs, misc, 20);
+    jacobi<NP>(A, V, n, rot, pairs, misc, 20, lda);
     if (op.block_stat) {
       if (tid == 0) {
         float mx = 0.f;
@@ -1199,7 +1210,7 @@ __global__ void __launch_bounds__(kLlrThreads, 1) llr_prox_wide_kernel(BlockSour
         Cch[q * W.t.ldch + rr] = x;
       }
       __syncthreads();
-      if (!identity) apply_W<NP, kWideTG>(Cch, W.t.ldch, rc, n, A);
+      if (!identity) apply_W<NP, kWideTG>(Cch, W.t.ldch, rc, n, A, lda);
       for (int e = tid; e < rc * n; e += blockDim.x) {
         const int q = e / rc, rr = e - q * rc, r = c0 + rr;
         store_elem(src, base, rows[r], rowph, r, q, qstride, Cch[q * W.t.ldch + rr]);
