@@ -233,8 +233,8 @@ def warm_start_headline(args, c, d) -> dict:
     x_zf, _, lam, energy, snap = W.reference(plain, d.y, args.ws_ref_iters, snapshot=True)
     codec = W.SubspaceCodec(mixed)
     net = Cnn.load(path)
-    W.warm_start_image(net, codec, x_zf, energy)                 # warm-up (workspace, attributes)
-    x0, net_ms = W.warm_start_image(net, codec, x_zf, energy)
+    W.warm_start_image(net, codec, x_zf, energy, d.y)            # warm-up (workspace, attributes)
+    x0, net_ms = W.warm_start_image(net, codec, x_zf, energy, d.y)
     net.close()
     targets = [1e-2, 1e-3]
     rp, cp = W.time_to_targets(plain, d.y, lam, x_zf, snap, targets, args.ws_ref_iters, chunk=10)

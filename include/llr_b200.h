@@ -347,14 +347,18 @@ int llr_cnn_loss_grad_dev(llr_cnn* net, const float* d_in, const float* d_target
 int llr_cnn_adam_step(llr_cnn* net, float lr, float beta1, float beta2, float eps, void* stream);
 int llr_cnn_train_step_dev(llr_cnn* net, const float* d_in, const float* d_target, const int32_t* dims,
                            float lr, double* loss, void* stream);
-/* CNN channels of subspace coefficients: chan[v][2k + {0,1}] = scale (re, im)(sum_q x[v + V q]
- * S[q + nq k]) (dti_subspace.rs:141-166), and the image back: x = (1/scale) c S^H, or
- * x += (1/scale) c S^H with accumulate != 0 (dti_subspace.rs:172-207).  Images in the
- * reference layout; 1 <= srank <= 16. */
+/* CNN channels of subspace coefficients: chan[v][2k + {0,1}] = scale (re, im)(sum_q u*[v + V q]
+ * x[v + V q] S[q + nq k]) (dti_subspace.rs:141-166), and the image back: x = u (1/scale) c S^H, or
+ * x += u (1/scale) c S^H with accumulate != 0 (dti_subspace.rs:172-207).  u is the unit phase of
+ * d_phase_ref (a reference image of the same shape, e.g. a low-resolution reconstruction; 0 maps
+ * to 1), or 1 when d_phase_ref is NULL: the demodulation that lets a real temporal subspace hold
+ * volumes that each carry their own smooth phase.  Images in the reference layout; 1 <= srank <= 16. */
 int llr_subspace_channels_dev(const llr_cf32* d_x, const int32_t* vol, int32_t nq, const llr_cf32* d_S,
-                              int32_t srank, float scale, float* d_chan, void* stream);
+                              int32_t srank, float scale, const llr_cf32* d_phase_ref, float* d_chan,
+                              void* stream);
 int llr_subspace_image_dev(const float* d_chan, const int32_t* vol, int32_t nq, const llr_cf32* d_S,
-                           int32_t srank, float scale, int32_t accumulate, llr_cf32* d_x, void* stream);
+                           int32_t srank, float scale, const llr_cf32* d_phase_ref, int32_t accumulate,
+                           llr_cf32* d_x, void* stream);
 
 #ifdef __cplusplus
 }

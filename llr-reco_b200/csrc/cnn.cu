@@ -532,9 +532,18 @@ __global__ void init_weights_kernel(float* __restrict__ W, int n, float stdv, ui
   }
 }
 
-// chan[v][2k + {0, 1}] = scale * (re, im) of sum_q x[v + V q] S[q + nq k]
+// Unit phase of a reference value (1 for 0): the demodulation factor of one voxel and volume.
+__device__ __forceinline__ float2 unit_phase(float2 r) {
+  const float m2 = r.x * r.x + r.y * r.y;
+  if (!(m2 > 0.f)) return make_float2(1.f, 0.f);
+  const float inv = rsqrtf(m2);
+  return make_float2(r.x * inv, r.y * inv);
+}
+
+// chan[v][2k + {0, 1}] = scale * (re, im) of sum_q u*[v + V q] x[v + V q] S[q + nq k], with u the unit
+// phase of the reference image `ph` (u = 1 when ph is null)
 __global__ void subspace_channels_kernel(const float2* __restrict__ x, long long V, int nq, const float2* __restrict__ S,
-                                         int r, float scale, float* __restrict__ chan) {
+                                         int r, float scale, const float2* __restrict__ ph, float* __restrict__ chan) {
   extern __shared__ float2 sS[];
   for (int i = threadIdx.x; i < nq * r; i += blockDim.x) sS[i] = S[i];
   __syncthreads();
@@ -543,7 +552,8 @@ __global__ void subspace_channels_kernel(const float2* __restrict__ x, long long
 #pragma unroll
     for (int k = 0; k < 16; ++k) c[k] = make_float2(0.f, 0.f);
     for (int q = 0; q < nq; ++q) {
-      const float2 xv = x[v + V * q];
+      float2 xv = x[v + V * q];
+      if (ph) xv = cmulc(unit_phase(ph[v + V * q]), xv);
 #pragma unroll
       for (int k = 0; k < 16; ++k)
         if (k < r) cfma(c[k], xv, sS[q + nq * k]);
@@ -557,9 +567,10 @@ __global__ void subspace_channels_kernel(const float2* __restrict__ x, long long
   }
 }
 
-// x[v + V q] (+)= (1 / scale) sum_k c_k conj(S[q + nq k])
+// x[v + V q] (+)= u[v + V q] (1 / scale) sum_k c_k conj(S[q + nq k]), u as above
 __global__ void subspace_image_kernel(const float* __restrict__ chan, long long V, int nq, const float2* __restrict__ S,
-                                      int r, float inv_scale, float2* __restrict__ x, int accumulate) {
+                                      int r, float inv_scale, const float2* __restrict__ ph, float2* __restrict__ x,
+                                      int accumulate) {
   extern __shared__ float2 sS[];
   for (int i = threadIdx.x; i < nq * r; i += blockDim.x) sS[i] = S[i];
   __syncthreads();
@@ -574,6 +585,7 @@ __global__ void subspace_image_kernel(const float* __restrict__ chan, long long 
 #pragma unroll
       for (int k = 0; k < 16; ++k)
         if (k < r) cfma_cb(acc, c[k], sS[q + nq * k]);
+      if (ph) acc = cmul(unit_phase(ph[v + V * q]), acc);
       if (accumulate) acc = cadd(acc, x[v + V * q]);
       x[v + V * q] = acc;
     }
@@ -895,25 +907,26 @@ int llr_cnn_train_step_dev(llr_cnn* n, const float* d_in, const float* d_target,
 }
 
 int llr_subspace_channels_dev(const llr_cf32* d_x, const int32_t* vol, int32_t nq, const llr_cf32* d_S, int32_t srank,
-                              float scale, float* d_chan, void* stream) {
+                              float scale, const llr_cf32* d_phase_ref, float* d_chan, void* stream) {
   if (!d_x || !vol || !d_S || !d_chan || nq < 1 || srank < 1 || srank > 16)
     return set_error(LLR_ERR_INVALID, "bad subspace channel arguments (1 <= srank <= 16)");
   const long long V = (long long)vol[0] * vol[1] * vol[2];
   note_launch();
   subspace_channels_kernel<<<grid_1d(V), 256, sizeof(float2) * nq * srank, (cudaStream_t)stream>>>(
-      (const float2*)d_x, V, nq, (const float2*)d_S, srank, scale, d_chan);
+      (const float2*)d_x, V, nq, (const float2*)d_S, srank, scale, (const float2*)d_phase_ref, d_chan);
   LLR_CUDA_TRY(cudaGetLastError());
   return LLR_OK;
 }
 
 int llr_subspace_image_dev(const float* d_chan, const int32_t* vol, int32_t nq, const llr_cf32* d_S, int32_t srank,
-                           float scale, int32_t accumulate, llr_cf32* d_x, void* stream) {
+                           float scale, const llr_cf32* d_phase_ref, int32_t accumulate, llr_cf32* d_x, void* stream) {
   if (!d_x || !vol || !d_S || !d_chan || nq < 1 || srank < 1 || srank > 16 || !(scale != 0.f))
     return set_error(LLR_ERR_INVALID, "bad subspace image arguments (1 <= srank <= 16, scale != 0)");
   const long long V = (long long)vol[0] * vol[1] * vol[2];
   note_launch();
   subspace_image_kernel<<<grid_1d(V), 256, sizeof(float2) * nq * srank, (cudaStream_t)stream>>>(
-      d_chan, V, nq, (const float2*)d_S, srank, 1.f / scale, (float2*)d_x, accumulate ? 1 : 0);
+      d_chan, V, nq, (const float2*)d_S, srank, 1.f / scale, (const float2*)d_phase_ref, (float2*)d_x,
+      accumulate ? 1 : 0);
   LLR_CUDA_TRY(cudaGetLastError());
   return LLR_OK;
 }

@@ -169,8 +169,8 @@ SIGNATURES = {
     "llr_cnn_loss_grad_dev": (C.c_int, [P, P, P, PI32, PF64, P]),
     "llr_cnn_adam_step": (C.c_int, [P, C.c_float, C.c_float, C.c_float, C.c_float, P]),
     "llr_cnn_train_step_dev": (C.c_int, [P, P, P, PI32, C.c_float, PF64, P]),
-    "llr_subspace_channels_dev": (C.c_int, [P, PI32, I32, P, I32, C.c_float, P, P]),
-    "llr_subspace_image_dev": (C.c_int, [P, PI32, I32, P, I32, C.c_float, I32, P, P]),
+    "llr_subspace_channels_dev": (C.c_int, [P, PI32, I32, P, I32, C.c_float, P, P, P]),
+    "llr_subspace_image_dev": (C.c_int, [P, PI32, I32, P, I32, C.c_float, P, I32, P, P]),
 }
 
 

@@ -141,14 +141,17 @@ class Cnn:
         return net
 
 
-def subspace_channels_dev(d_x, vol, nq: int, d_S, srank: int, scale: float, out: DeviceArray) -> None:
-    """CNN channels scale * (x S) of a device image in the reference layout."""
-    check(lib.llr_subspace_channels_dev(d_x, _i32(vol), int(nq), d_S, int(srank), float(scale), out.ptr, None))
+def subspace_channels_dev(d_x, vol, nq: int, d_S, srank: int, scale: float, out: DeviceArray,
+                          d_phase_ref=None) -> None:
+    """CNN channels scale * ((u* x) S) of a device image in the reference layout; u is the unit
+    phase of the device image ``d_phase_ref`` (1 when None)."""
+    check(lib.llr_subspace_channels_dev(d_x, _i32(vol), int(nq), d_S, int(srank), float(scale), d_phase_ref,
+                                        out.ptr, None))
 
 
 def subspace_image_dev(chan: DeviceArray, vol, nq: int, d_S, srank: int, scale: float, d_x,
-                       accumulate: bool = False) -> None:
-    """Image (1 / scale) c S^H from CNN channels into a device image (reference layout); added
+                       accumulate: bool = False, d_phase_ref=None) -> None:
+    """Image u (1 / scale) c S^H from CNN channels into a device image (reference layout); added
     to what the image holds when ``accumulate``."""
-    check(lib.llr_subspace_image_dev(chan.ptr, _i32(vol), int(nq), d_S, int(srank), float(scale),
+    check(lib.llr_subspace_image_dev(chan.ptr, _i32(vol), int(nq), d_S, int(srank), float(scale), d_phase_ref,
                                      1 if accumulate else 0, d_x, None))

@@ -42,6 +42,7 @@ class Protocol:
     recon_seed: int = 3
     fixed_partition: bool = True
     gram_mode: int = 0
+    demodulate: bool = True     # channels of the phase-demodulated image (phase of the calibration image)
 
     @property
     def nq(self) -> int:
@@ -82,6 +83,30 @@ def reference(proto: Protocol, y: np.ndarray, n_iter: int, snapshot: bool = Fals
         return x_zf, ctx.download_image(), lam, energy
 
 
+def calibration_kspace(proto: Protocol, y: np.ndarray) -> np.ndarray:
+    """The fully sampled k-space centre of y (|ky - ny/2|, |kz - nz/2| < centre/2, every x), zero
+    elsewhere."""
+    nx, ny, nz, nq = y.shape
+    h = proto.centre // 2
+    yc = np.zeros(y.shape, dtype=np.complex64, order="F")
+    sl = (slice(None), slice(ny // 2 - h, ny // 2 + h), slice(nz // 2 - h, nz // 2 + h), slice(None))
+    yc[sl] = y[sl]
+    return yc
+
+
+def calibration_image(proto: Protocol, y: np.ndarray) -> Optional[DeviceBuffer]:
+    """Device image A^H of the calibration k-space: a low-resolution reconstruction whose phase is
+    the smooth phase of each volume.  The network works on the temporal-subspace coefficients of
+    the image demodulated by this phase, since every volume carries its own phase and a real
+    subspace cannot hold it (None: no demodulation)."""
+    if not proto.demodulate:
+        return None
+    d = DeviceBuffer.from_array(calibration_kspace(proto, y))
+    check(lib.llr_signal_model_dev(d.ptr, L.i32x3(proto.vol), proto.nq, None, None, L.LLR_INVERSE, None))
+    check(lib.llr_stream_sync(None))
+    return d
+
+
 def channel_scale(proto: Protocol, energy: float) -> float:
     """Unit-RMS channels: the coefficients carry about the image energy (A is unitary)."""
     V = int(np.prod(proto.vol))
@@ -96,19 +121,19 @@ class SubspaceCodec:
         self.S = proto.subspace() if S is None else S
         self.dS = DeviceBuffer.from_array(np.asfortranarray(self.S.astype(np.complex64)))
 
-    def channels(self, x: np.ndarray, scale: float) -> DeviceArray:
+    def channels(self, x: np.ndarray, scale: float, ph: Optional[DeviceBuffer] = None) -> DeviceArray:
         p = self.proto
         dx = DeviceBuffer.from_array(x.astype(np.complex64))
         out = DeviceArray((p.vol[2], p.vol[1], p.vol[0], 2 * p.srank))
-        subspace_channels_dev(dx.ptr, p.vol, p.nq, self.dS.ptr, p.srank, scale, out)
+        subspace_channels_dev(dx.ptr, p.vol, p.nq, self.dS.ptr, p.srank, scale, out, ph.ptr if ph else None)
         check(lib.llr_stream_sync(None))
         dx.close()
         return out
 
-    def image(self, chan: DeviceArray, scale: float) -> np.ndarray:
+    def image(self, chan: DeviceArray, scale: float, ph: Optional[DeviceBuffer] = None) -> np.ndarray:
         p = self.proto
         dx = DeviceBuffer(8 * int(np.prod(p.vol)) * p.nq)
-        subspace_image_dev(chan, p.vol, p.nq, self.dS.ptr, p.srank, scale, dx.ptr)
+        subspace_image_dev(chan, p.vol, p.nq, self.dS.ptr, p.srank, scale, dx.ptr, d_phase_ref=ph.ptr if ph else None)
         out = dx.download(np.empty(tuple(p.vol) + (p.nq,), dtype=np.complex64, order="F"))
         dx.close()
         return out
@@ -121,7 +146,10 @@ def training_pairs(proto: Protocol, codec: SubspaceCodec, seeds: Sequence[int], 
         d = proto.subject(s)
         x_zf, x_ref, _, energy = reference(proto, d.y, n_ref)
         sc = channel_scale(proto, energy)
-        pairs.append((codec.channels(x_zf, sc), codec.channels(x_ref, sc)))
+        ph = calibration_image(proto, d.y)
+        pairs.append((codec.channels(x_zf, sc, ph), codec.channels(x_ref, sc, ph)))
+        if ph is not None:
+            ph.close()
     return pairs
 
 
@@ -141,27 +169,34 @@ def train(net: Cnn, pairs, epochs: int, lr: float, lr_final: Optional[float] = N
     return losses
 
 
-def warm_start_image(net: Cnn, codec: SubspaceCodec, x_zf: np.ndarray, energy: float):
-    """Network start image x0 = x_zf + (c_out - c_in) S^H / scale -- the network corrects the
-    subspace part of the zero-filled image and keeps the rest -- and the milliseconds of device
-    work producing it, measured between stream synchronisations; host copies are outside."""
+def warm_start_image(net: Cnn, codec: SubspaceCodec, x_zf: np.ndarray, energy: float, y: np.ndarray):
+    """Network start image x0 = x_zf + u (c_out - c_in) S^H / scale -- the network corrects the
+    demodulated subspace part of the zero-filled image and keeps the rest; u is the unit phase of
+    the calibration image -- and the milliseconds of device work producing it (calibration image,
+    channels, network, image), measured between stream synchronisations; host copies are outside."""
     import time
     p = codec.proto
     sc = channel_scale(p, energy)
     dx = DeviceBuffer.from_array(x_zf.astype(np.complex64))
     chan = DeviceArray((p.vol[2], p.vol[1], p.vol[0], 2 * p.srank))
     out = DeviceArray(chan.shape)
+    # host masking and upload of the calibration lines are data preparation (outside the timing)
+    dc = DeviceBuffer.from_array(calibration_kspace(p, y)) if p.demodulate else None
     check(lib.llr_stream_sync(None))
     t0 = time.perf_counter()
-    subspace_channels_dev(dx.ptr, p.vol, p.nq, codec.dS.ptr, p.srank, sc, chan)
+    if dc is not None:
+        check(lib.llr_signal_model_dev(dc.ptr, L.i32x3(p.vol), p.nq, None, None, L.LLR_INVERSE, None))
+    ph = dc.ptr if dc is not None else None
+    subspace_channels_dev(dx.ptr, p.vol, p.nq, codec.dS.ptr, p.srank, sc, chan, ph)
     net.forward_dev(chan, out)
-    subspace_image_dev(out, p.vol, p.nq, codec.dS.ptr, p.srank, sc, dx.ptr, accumulate=True)
-    subspace_image_dev(chan, p.vol, p.nq, codec.dS.ptr, p.srank, -sc, dx.ptr, accumulate=True)
+    subspace_image_dev(out, p.vol, p.nq, codec.dS.ptr, p.srank, sc, dx.ptr, accumulate=True, d_phase_ref=ph)
+    subspace_image_dev(chan, p.vol, p.nq, codec.dS.ptr, p.srank, -sc, dx.ptr, accumulate=True, d_phase_ref=ph)
     check(lib.llr_stream_sync(None))
     ms = 1e3 * (time.perf_counter() - t0)
     x0 = dx.download(np.empty_like(x_zf, dtype=np.complex64, order="F"))
-    for b in (dx, chan, out):
-        b.close()
+    for b in (dx, chan, out, dc):
+        if b is not None:
+            b.close()
     return x0, ms
 
 

@@ -68,6 +68,18 @@ def test_subspace_channels_and_image_match_oracle(gpu):
     subspace_image_dev(ch, vol, nq, dS.ptr, r, 3.0, dy.ptr)
     back = dy.download(np.empty_like(x, order="F"))
     assert rel_err(back, CO.subspace_image(got.astype(np.float64), S.astype(np.complex128), 3.0)) < 1e-6
+    # demodulated by the unit phase u of a reference image: channels of u* x, image u (c S^H)
+    ref = (rng.standard_normal(vol + (nq,)) + 1j * rng.standard_normal(vol + (nq,))).astype(np.complex64)
+    ref[0, 0, 0, 0] = 0                                           # a zero reference maps to u = 1
+    u = np.where(ref == 0, 1.0, ref / np.maximum(np.abs(ref), 1e-30))
+    dref = DeviceBuffer.from_array(ref)
+    subspace_channels_dev(dx.ptr, vol, nq, dS.ptr, r, 3.0, ch, dref.ptr)
+    llr_b200._lib.check(llr_b200._lib.lib.llr_stream_sync(None))
+    gotp = ch.numpy()
+    assert rel_err(gotp, CO.subspace_channels(np.conj(u) * x.astype(np.complex128), S.astype(np.complex128), 3.0)) < 1e-6
+    subspace_image_dev(ch, vol, nq, dS.ptr, r, 3.0, dy.ptr, d_phase_ref=dref.ptr)
+    backp = dy.download(np.empty_like(x, order="F"))
+    assert rel_err(backp, u * CO.subspace_image(gotp.astype(np.float64), S.astype(np.complex128), 3.0)) < 1e-6
 
 
 def _adam_oracle(p, x, t, steps, lr, b1=0.9, b2=0.999, eps=1e-8):
@@ -129,7 +141,7 @@ def test_learned_warm_start_gain(gpu):
         assert losses[-1] < 0.8 * losses[0]
         d = proto.subject(977)
         x_zf, x_ref, lam, energy, snap = W.reference(proto, d.y, 1600, snapshot=True)
-        x0, ms = W.warm_start_image(net, codec, x_zf, energy)
+        x0, ms = W.warm_start_image(net, codec, x_zf, energy, d.y)
     e_zf, e_ws = W.nrmse(x_zf, x_ref), W.nrmse(x0, x_ref)
     assert e_ws < e_zf, (e_ws, e_zf)
     plain, cp = W.time_to_targets(proto, d.y, lam, x_zf, snap, [3e-2, 1e-9], 200)
