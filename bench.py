@@ -471,6 +471,40 @@ def run_reference(args, dist: Dist) -> None:
     print(json.dumps(out))
 
 
+def cnn_timing(args) -> None:
+    """Device time of the warm-start network (forward; loss and gradients) on random channels at
+    96^3 and at the config-2 geometry, between stream synchronisations."""
+    from llr_b200.cnn import Cnn, DeviceArray
+    from llr_b200 import _lib as L
+    res = {}
+    for dims in [(96, 96, 96), (96, 192, 192)]:
+        net = Cnn(seed=1)
+        rng = np.random.default_rng(0)
+        x = DeviceArray.from_numpy(rng.standard_normal(dims + (14,)).astype(np.float32))
+        t = DeviceArray.from_numpy(rng.standard_normal(dims + (14,)).astype(np.float32))
+        o = DeviceArray(dims + (14,))
+        for _ in range(2):
+            net.forward_dev(x, o)
+        L.check(L.lib.llr_stream_sync(None))
+        t0 = time.perf_counter()
+        for _ in range(5):
+            net.forward_dev(x, o)
+        L.check(L.lib.llr_stream_sync(None))
+        fwd = (time.perf_counter() - t0) / 5 * 1e3
+        net.loss_grad_dev(x, t)
+        t0 = time.perf_counter()
+        for _ in range(3):
+            net.loss_grad_dev(x, t)
+        L.check(L.lib.llr_stream_sync(None))
+        fb = (time.perf_counter() - t0) / 3 * 1e3
+        flops = 2 * 27 * (14 * 32 + 6 * 32 * 32 + 32 * 14) * dims[0] * dims[1] * dims[2]
+        res["x".join(map(str, dims[::-1]))] = {"forward_ms": round(fwd, 3), "forward_tflops": round(flops / fwd / 1e9, 2),
+                                               "loss_grad_ms": round(fb, 3),
+                                               "loss_grad_tflops": round(3 * flops / fb / 1e9, 2)}
+        net.close()
+    print(json.dumps({"cnn_timing": res}))
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -499,7 +533,11 @@ def main(argv=None):
     ap.add_argument("--traffic-kernels", default="llr_gram_tc|llr_eig_warp|llr_apply")
     ap.add_argument("--traffic-scale", type=float, default=1.0)
     ap.add_argument("--traffic-captured-on", default=None)
+    ap.add_argument("--cnn-timing", action="store_true", help="time the warm-start network and exit")
     args = ap.parse_args(argv)
+    if args.cnn_timing:
+        cnn_timing(args)
+        return
     if args.ncu_traffic:
         write_traffic(args)
         return
