@@ -418,6 +418,7 @@ def run_b200(args, dist: Dist) -> None:
             "path": "hybrid (x-transform eliminated: line-structured sampling)",
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "warm_start": headline,
             "gpu_launches": n_kernels * args.steps,
+            "jacobi_fallback_blocks_last_iteration": ctx.fallback_blocks,
             "residual_first_last": [float(hist[0]), float(hist[-1])],
         }
         print(json.dumps(out))
