@@ -269,7 +269,7 @@ static int wavelet_pass(llr_ctx* c, cudaStream_t s, float store_scale, bool in_i
                                          std::min(nb, sr - k0), c->cfg.wavelet_alpha, c->d_wavelet_work, none,
                                          nullptr, 0, 1.f, s));
     return launch_subspace_expand(c->d_work, c->d_x, c->d_S, sr, c->g, ctx_phase(c, c->d_ph_ksp, !c->hybrid), 1,
-                                  store_scale, s);
+                                  c->ph_uniform, store_scale, s);
   }
   const int nb = std::max(1, (int)(c->wavelet_work_elems / wavelet_workspace_elems(c->wplan, 1)));
   PhaseTab ph = ctx_phase(c, c->d_ph_ksp, !c->hybrid);

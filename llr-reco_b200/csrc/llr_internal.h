@@ -98,7 +98,7 @@ struct SubspaceOp {
 int launch_llr_prox_subspace(const BlockSource& src, const SubspaceOp& op, cudaStream_t stream);
 // x(., q) = (sum_k c(., k) conj(S[q, k])) * phase(q, .) * scale, planar volumes (nq from srank)
 int launch_subspace_expand(const float2* coef, float2* x, const float2* S, int srank, const Geom& g, PhaseTab ph,
-                           int store_phase, float scale, cudaStream_t s);
+                           int store_phase, int ph_uniform, float scale, cudaStream_t s);
 
 // layout / transform kernels (signal_model.cu)
 int launch_ref_to_planar(const float2* ref, float2* planar, const Geom& g, float scale, PhaseTab ph,

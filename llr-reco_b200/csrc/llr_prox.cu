@@ -266,10 +266,11 @@ __global__ void __launch_bounds__(kLlrThreads) llr_subspace_coef_kernel(BlockSou
       for (int k = 0; k < kSubMax; ++k) z[k] = make_float2(0.f, 0.f);
       int ix = 0, iy = 0, iz = 0;
       block_row_coord(src, blk, sh, r, ix, iy, iz);
+      const float2 p0 = phase_at(src.ph, src.g, 0, ix, iy, iz);   // every volume's, when uniform
 #pragma unroll 4
       for (int q = 0; q < nq; ++q) {
         float2 v = src.data[planar_index(src.g, ix, iy, iz, q)];
-        v = cscale(cmul_bc(v, phase_at(src.ph, src.g, q, ix, iy, iz)), src.load_scale);
+        v = cscale(cmul_bc(v, src.ph_uniform ? p0 : phase_at(src.ph, src.g, q, ix, iy, iz)), src.load_scale);
 #pragma unroll
         for (int k = 0; k < kSubMax; ++k)
           if (k < sr) cfma(z[k], v, Ss[q * sr + k]);
@@ -295,7 +296,8 @@ __global__ void __launch_bounds__(kLlrThreads) llr_subspace_coef_kernel(BlockSou
 
 __global__ void __launch_bounds__(256) subspace_expand_kernel(const float2* __restrict__ coef, float2* __restrict__ x,
                                                               const float2* __restrict__ S, int srank, Geom g,
-                                                              PhaseTab ph, int store_phase, float scale) {
+                                                              PhaseTab ph, int store_phase, int ph_uniform,
+                                                              float scale) {
   __shared__ float2 Ss[64 * kSubMax];
   for (int i = threadIdx.x; i < g.nq * srank; i += blockDim.x) Ss[i] = S[i];   // column-major (q, k)
   __syncthreads();
@@ -306,15 +308,16 @@ __global__ void __launch_bounds__(256) subspace_expand_kernel(const float2* __re
     const int iy = (int)(v % g.ny);
     const long long r = v / g.ny;
     const int iz = (int)(r % g.nz), ix = (int)(r / g.nz);
+    // the stored value's factor: scale times the phase (computed once when every volume shares it)
+    const float2 f0 = cscale(store_phase ? phase_at(ph, g, 0, ix, iy, iz) : make_float2(1.f, 0.f), scale);
 #pragma unroll 4
     for (int q = 0; q < g.nq; ++q) {
       float2 a = make_float2(0.f, 0.f);
 #pragma unroll
       for (int k = 0; k < kSubMax; ++k)
         if (k < srank) cfma_cb(a, c[k], Ss[q + g.nq * k]);
-      a = cscale(a, scale);
-      if (store_phase) a = cmul(a, phase_at(ph, g, q, ix, iy, iz));
-      x[v + g.V * q] = a;
+      const float2 f = (ph_uniform || !store_phase) ? f0 : cscale(phase_at(ph, g, q, ix, iy, iz), scale);
+      x[v + g.V * q] = cmul(a, f);
     }
   }
 }
@@ -397,11 +400,11 @@ int launch_lift(const float2* vol, float2* mat, const int* vs, int nq, const int
 // rhsCdgmmBatched (kernels.cu:11-67) and a batched complex GEMM with the semantics of
 // cublas_cgemm_strided_batched_device (cublas.rs:12-105).
 int launch_subspace_expand(const float2* coef, float2* x, const float2* S, int srank, const Geom& g, PhaseTab ph,
-                           int store_phase, float scale, cudaStream_t s) {
+                           int store_phase, int ph_uniform, float scale, cudaStream_t s) {
   if (srank < 1 || srank > kSubMax || g.nq > 64) return set_error(LLR_ERR_UNSUPPORTED, "subspace expand shape");
   const long long blocks = std::min<long long>((g.V + 255) / 256, 148LL * 16);
   note_launch();
-  subspace_expand_kernel<<<(unsigned)blocks, 256, 0, s>>>(coef, x, S, srank, g, ph, store_phase, scale);
+  subspace_expand_kernel<<<(unsigned)blocks, 256, 0, s>>>(coef, x, S, srank, g, ph, store_phase, ph_uniform, scale);
   LLR_CUDA_TRY(cudaGetLastError());
   return LLR_OK;
 }
