@@ -153,7 +153,7 @@ namespace {
 
 constexpr int kSubMax = 16;   // max subspace rank
 
-template <int NPMAX>
+template <int NPMAX, int KM>
 __global__ void __launch_bounds__(kLlrThreads) llr_subspace_kernel(BlockSource src, SubspaceOp op, SmemLayout L) {
   extern __shared__ __align__(16) unsigned char smem[];
   Misc* misc = reinterpret_cast<Misc*>(smem);
@@ -181,9 +181,9 @@ __global__ void __launch_bounds__(kLlrThreads) llr_subspace_kernel(BlockSource s
   for (long long blk = blockIdx.x; blk < src.nblocks; blk += gridDim.x) {
     // Z[r, k] = sum_q X[r, q] S[q, k]
     for (int r = threadIdx.x; r < m; r += blockDim.x) {
-      float2 z[kSubMax];
+      float2 z[KM];
 #pragma unroll
-      for (int k = 0; k < kSubMax; ++k) z[k] = make_float2(0.f, 0.f);
+      for (int k = 0; k < KM; ++k) z[k] = make_float2(0.f, 0.f);
       int ix = 0, iy = 0, iz = 0;
       if (src.kind == 1) block_row_coord(src, blk, sh, r, ix, iy, iz);
       for (int q = 0; q < nq; ++q) {
@@ -195,11 +195,11 @@ __global__ void __launch_bounds__(kLlrThreads) llr_subspace_kernel(BlockSource s
           v = cscale(cmul_bc(v, phase_at(src.ph, src.g, q, ix, iy, iz)), src.load_scale);
         }
 #pragma unroll
-        for (int k = 0; k < kSubMax; ++k)
+        for (int k = 0; k < KM; ++k)
           if (k < sr) cfma(z[k], v, Ss[q * sr + k]);
       }
 #pragma unroll
-      for (int k = 0; k < kSubMax; ++k)
+      for (int k = 0; k < KM; ++k)
         if (k < sr) Z[k * L.ldc + r] = z[k];
     }
     __syncthreads();
@@ -210,15 +210,15 @@ __global__ void __launch_bounds__(kLlrThreads) llr_subspace_kernel(BlockSource s
     apply_W<NPMAX, 2>(Z, L.ldc, m, sr, A);
     // X'[r, q] = sum_k Z'[r, k] conj(S[q, k])
     for (int r = threadIdx.x; r < m; r += blockDim.x) {
-      float2 z[kSubMax];
+      float2 z[KM];
 #pragma unroll
-      for (int k = 0; k < kSubMax; ++k) z[k] = (k < sr) ? Z[k * L.ldc + r] : make_float2(0.f, 0.f);
+      for (int k = 0; k < KM; ++k) z[k] = (k < sr) ? Z[k * L.ldc + r] : make_float2(0.f, 0.f);
       int ix = 0, iy = 0, iz = 0;
       if (src.kind == 1) block_row_coord(src, blk, sh, r, ix, iy, iz);
       for (int q = 0; q < nq; ++q) {
         float2 v = make_float2(0.f, 0.f);
 #pragma unroll
-        for (int k = 0; k < kSubMax; ++k)
+        for (int k = 0; k < KM; ++k)
           if (k < sr) cfma_cb(v, z[k], Ss[q * sr + k]);
         if (src.kind == 0) {
           src.data[blk * (long long)m * nq + (long long)q * m + r] = v;
@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(kLlrThreads) llr_subspace_kernel(BlockSource s
 
 // Coefficient output: the same gather and low-rank step, storing Z' = LR(X S) as srank
 // planar coefficient volumes (image space) for a shrink in the coefficient domain.
-template <int NPMAX>
+template <int NPMAX, int KM>
 __global__ void __launch_bounds__(kLlrThreads) llr_subspace_coef_kernel(BlockSource src, SubspaceOp op, SmemLayout L) {
   extern __shared__ __align__(16) unsigned char smem[];
   Misc* misc = reinterpret_cast<Misc*>(smem);
@@ -261,9 +261,9 @@ __global__ void __launch_bounds__(kLlrThreads) llr_subspace_coef_kernel(BlockSou
   gc.nq = sr;
   for (long long blk = blockIdx.x; blk < src.nblocks; blk += gridDim.x) {
     for (int r = threadIdx.x; r < m; r += blockDim.x) {
-      float2 z[kSubMax];
+      float2 z[KM];
 #pragma unroll
-      for (int k = 0; k < kSubMax; ++k) z[k] = make_float2(0.f, 0.f);
+      for (int k = 0; k < KM; ++k) z[k] = make_float2(0.f, 0.f);
       int ix = 0, iy = 0, iz = 0;
       block_row_coord(src, blk, sh, r, ix, iy, iz);
       const float2 p0 = phase_at(src.ph, src.g, 0, ix, iy, iz);   // every volume's, when uniform
@@ -272,11 +272,11 @@ __global__ void __launch_bounds__(kLlrThreads) llr_subspace_coef_kernel(BlockSou
         float2 v = src.data[planar_index(src.g, ix, iy, iz, q)];
         v = cscale(cmul_bc(v, src.ph_uniform ? p0 : phase_at(src.ph, src.g, q, ix, iy, iz)), src.load_scale);
 #pragma unroll
-        for (int k = 0; k < kSubMax; ++k)
+        for (int k = 0; k < KM; ++k)
           if (k < sr) cfma(z[k], v, Ss[q * sr + k]);
       }
 #pragma unroll
-      for (int k = 0; k < kSubMax; ++k)
+      for (int k = 0; k < KM; ++k)
         if (k < sr) Z[k * L.ldc + r] = z[k];
     }
     __syncthreads();
@@ -294,6 +294,7 @@ __global__ void __launch_bounds__(kLlrThreads) llr_subspace_coef_kernel(BlockSou
   }
 }
 
+template <int KM>
 __global__ void __launch_bounds__(256) subspace_expand_kernel(const float2* __restrict__ coef, float2* __restrict__ x,
                                                               const float2* __restrict__ S, int srank, Geom g,
                                                               PhaseTab ph, int store_phase, int ph_uniform,
@@ -302,9 +303,9 @@ __global__ void __launch_bounds__(256) subspace_expand_kernel(const float2* __re
   for (int i = threadIdx.x; i < g.nq * srank; i += blockDim.x) Ss[i] = S[i];   // column-major (q, k)
   __syncthreads();
   for (long long v = blockIdx.x * 256LL + threadIdx.x; v < g.V; v += (long long)gridDim.x * 256) {
-    float2 c[kSubMax];
+    float2 c[KM];
 #pragma unroll
-    for (int k = 0; k < kSubMax; ++k) c[k] = k < srank ? coef[v + g.V * k] : make_float2(0.f, 0.f);
+    for (int k = 0; k < KM; ++k) c[k] = k < srank ? coef[v + g.V * k] : make_float2(0.f, 0.f);
     const int iy = (int)(v % g.ny);
     const long long r = v / g.ny;
     const int iz = (int)(r % g.nz), ix = (int)(r / g.nz);
@@ -314,7 +315,7 @@ __global__ void __launch_bounds__(256) subspace_expand_kernel(const float2* __re
     for (int q = 0; q < g.nq; ++q) {
       float2 a = make_float2(0.f, 0.f);
 #pragma unroll
-      for (int k = 0; k < kSubMax; ++k)
+      for (int k = 0; k < KM; ++k)
         if (k < srank) cfma_cb(a, c[k], Ss[q + g.nq * k]);
       const float2 f = (ph_uniform || !store_phase) ? f0 : cscale(phase_at(ph, g, q, ix, iy, iz), scale);
       x[v + g.V * q] = cmul(a, f);
@@ -332,7 +333,9 @@ int launch_llr_prox_subspace(const BlockSource& src, const SubspaceOp& op, cudaS
   L.total = align16(L.total + sizeof(float2) * (size_t)op.nq * op.srank);
   if (L.total > 227 * 1024) return set_error(LLR_ERR_UNSUPPORTED, "subspace prox needs %zu B smem", L.total);
   if (op.coef_out && src.kind != 1) return set_error(LLR_ERR_INVALID, "coefficient output needs volume blocks");
-  auto kern = op.coef_out ? llr_subspace_coef_kernel<16> : llr_subspace_kernel<16>;
+  // per-thread coefficient registers sized to the rank class (fewer registers, more CTAs per SM)
+  auto kern = op.coef_out ? (op.srank <= 8 ? llr_subspace_coef_kernel<16, 8> : llr_subspace_coef_kernel<16, 16>)
+                          : (op.srank <= 8 ? llr_subspace_kernel<16, 8> : llr_subspace_kernel<16, 16>);
   LLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total));
     LLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   int dev = 0, nsm = 0, occ = 0;
@@ -404,7 +407,11 @@ int launch_subspace_expand(const float2* coef, float2* x, const float2* S, int s
   if (srank < 1 || srank > kSubMax || g.nq > 64) return set_error(LLR_ERR_UNSUPPORTED, "subspace expand shape");
   const long long blocks = std::min<long long>((g.V + 255) / 256, 148LL * 16);
   note_launch();
-  subspace_expand_kernel<<<(unsigned)blocks, 256, 0, s>>>(coef, x, S, srank, g, ph, store_phase, ph_uniform, scale);
+  if (srank <= 8)
+    subspace_expand_kernel<8><<<(unsigned)blocks, 256, 0, s>>>(coef, x, S, srank, g, ph, store_phase, ph_uniform, scale);
+  else
+    subspace_expand_kernel<16><<<(unsigned)blocks, 256, 0, s>>>(coef, x, S, srank, g, ph, store_phase, ph_uniform,
+                                                                scale);
   LLR_CUDA_TRY(cudaGetLastError());
   return LLR_OK;
 }
