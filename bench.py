@@ -478,7 +478,7 @@ def cnn_timing(args) -> None:
     from llr_b200.cnn import Cnn, DeviceArray
     from llr_b200 import _lib as L
     res = {}
-    for dims in [(96, 96, 96), (96, 192, 192)]:
+    for dims in ([tuple(args.cnn_dims[::-1])] if args.cnn_dims else [(96, 96, 96), (96, 192, 192)]):
         net = Cnn(seed=1)
         rng = np.random.default_rng(0)
         x = DeviceArray.from_numpy(rng.standard_normal(dims + (14,)).astype(np.float32))
@@ -535,6 +535,7 @@ def main(argv=None):
     ap.add_argument("--traffic-scale", type=float, default=1.0)
     ap.add_argument("--traffic-captured-on", default=None)
     ap.add_argument("--cnn-timing", action="store_true", help="time the warm-start network and exit")
+    ap.add_argument("--cnn-dims", type=int, nargs=3, metavar=("NX", "NY", "NZ"), help="one volume for --cnn-timing")
     args = ap.parse_args(argv)
     if args.cnn_timing:
         cnn_timing(args)
