@@ -19,6 +19,8 @@
 #include <vector>
 #include <algorithm>
 
+#include <cuda_bf16.h>
+
 #include "llr_common.cuh"
 #include "llr_internal.h"
 #include "llr_umma.cuh"
@@ -66,35 +68,59 @@ __host__ __device__ __forceinline__ uint16_t f32_to_bf16(float f) {
 }
 
 // ---------------------------------------------------------------------------------------
-// conv3d as an implicit GEMM on the tensor cores (tcgen05, TF32 with FP32 accumulation in
-// tensor memory).  A CTA owns tiles of 128 output voxels (8 x 4 x 4); per tile the halo
-// (10 x 6 x 6 voxels, all input channels) is staged once in shared memory, then for each of
-// the 27 taps the 128 x CIN operand (the tap-shifted voxels) is split into TF32 hi + lo planes
-// in the 128-byte swizzled K-major layout and multiplied with that tap's weights (BF16, exact
-// in TF32; all 27 taps resident in shared memory, N = COUT padded to 16 / 32, K = CIN padded
-// to 32).  D[voxel][co] += hi W + lo W keeps FP32-level accuracy (the split error of x is
-// ~2^-22 relative).  Two operand buffers: the planes of tap t + 1 are written while the tensor
-// core works on tap t; one elected thread issues the MMAs and commits them to mbarriers with
-// bounded waits.  Epilogue: tcgen05.ld of the accumulator, bias, ReLU, residual, store.
+// Geometry shared by the tensor-core conv kernels.
 // ---------------------------------------------------------------------------------------
 constexpr int kCvThreads = 256;
-constexpr int kCvTX = 8, kCvTY = 4, kCvTZ = 4;                  // 128 output voxels per tile
+constexpr int kCvTX = 8, kCvTY = 4, kCvTZ = 4;                  // weight-gradient tile: 128 voxels
 constexpr int kCvHX = kCvTX + 2, kCvHY = kCvTY + 2, kCvHZ = kCvTZ + 2;
 constexpr int kCvHV = kCvHX * kCvHY * kCvHZ;
 constexpr int kCvPlane = 128 * 128;                              // one 128 x 32 TF32 operand plane (bytes)
 
 __host__ __device__ constexpr int cv_np(int cout) { return cout <= 16 ? 16 : 32; }
 
+// ---------------------------------------------------------------------------------------
+// conv3d forward (and backward-data: the same convolution with W') as an implicit GEMM on
+// the tensor cores, tcgen05 kind::f16 with BF16 operands and FP32 accumulation in tensor
+// memory.
+//
+// A CTA owns tiles of 128 output voxels, 8 (x) x 16 (y) x 1 (z); row a = x + 8 y of the
+// 128 x COUT accumulator.  The tile's input halo (10 x 18 x 3 voxels, all channels) is
+// written once into shared memory in the unswizzled K-major operand layout: channel chunk c
+// (8 BF16 = 16 B) of halo voxel h at byte c * CS + 16 h.  The operand of tap (dx, dy, dz) is
+// then the same array read from voxel dx + 10 (dy + 18 dz) on: 8 consecutive x form one core
+// matrix (128 contiguous bytes), the 16 rows y step by 10 voxels (SBO = 160 B) and the K
+// chunks by CS (LBO).  There is no per-tap copy and no per-tap barrier: once the halo is in
+// place one thread issues the MMAs of all 27 taps back to back.
+//
+// FP32 accuracy: each activation is split x = b1 + b2 + b3 into three BF16 planes (b1 the
+// BF16 rounding of x, b2 of x - b1, b3 of the rest: ~24 significant bits in all); the weights
+// are BF16 and exact.  D += b1 W + b2 W + b3 W, three MMAs per K step of 16 channels.
+//
+// Pipeline: the next tile's FP32 halo is copied with cp.async (zero fill outside the volume
+// and for padding channels) into a staging buffer while the current tile's MMAs run, and two
+// accumulators in tensor memory let the epilogue of tile i - 1 (tcgen05.ld, bias, ReLU,
+// residual, store) run beside the MMAs of tile i.  Every mbarrier wait is bounded; one that
+// runs out sets the error flag and the CTA stops.
+// ---------------------------------------------------------------------------------------
+constexpr int kFwTX = 8, kFwTY = 16;                             // forward tile: 128 voxels of one z plane
+constexpr int kFwHX = kFwTX + 2, kFwHY = kFwTY + 2, kFwHZ = 3;
+constexpr int kFwNV = kFwHX * kFwHY * kFwHZ;                       // 540 halo voxels
+constexpr int kFwCS = kFwNV * 16;                                  // bytes of one 8-channel chunk of a plane
+
 template <int CIN, int COUT>
 struct CvLayout {
-  static constexpr int NP = cv_np(COUT);
-  static constexpr int HP = (CIN + 3) & ~3;                        // halo channel pitch: 16-byte rows
-  static constexpr int NCH = HP / 4;                               // 16-byte channel chunks per voxel
-  static constexpr size_t off_hdr = 0;                             // 3 mbarriers + TMEM address
-  static constexpr size_t off_w = 1024;                            // 27 tap blocks of NP x 128 B
-  static constexpr size_t off_a = off_w + (size_t)27 * NP * 128;   // 2 buffers x (hi, lo)
-  static constexpr size_t off_halo = off_a + (size_t)4 * kCvPlane;
-  static constexpr size_t total = off_halo + sizeof(float) * (size_t)kCvHV * HP;
+  static constexpr int NP = cv_np(COUT);                           // accumulator columns (N)
+  static constexpr int KC = (CIN + 15) / 16 * 2;                   // 8-channel chunks, K padded to 16
+  static constexpr int KS = KC / 2;                                // K steps of 16 channels per tap
+  static constexpr int RC = 2 * KC;                                // 4-channel chunks of the FP32 halo
+  static constexpr int NPL = 3;                                    // BF16 planes per activation
+  static constexpr int WT = KC * NP * 16;                          // bytes of one tap's weights
+  static constexpr size_t PB = (size_t)KC * kFwCS;                 // bytes of one BF16 plane
+  static constexpr size_t off_hdr = 0;                             // mbarriers, TMEM address
+  static constexpr size_t off_pl = 1024;                           // NPL BF16 planes
+  static constexpr size_t off_w = off_pl + NPL * PB;               // 27 taps of weights
+  static constexpr size_t off_raw = off_w + (size_t)27 * WT;       // FP32 halo staging, chunk r at r NV 16
+  static constexpr size_t total = off_raw + (size_t)RC * kFwNV * 16;
 };
 
 struct CvGeo {
@@ -102,171 +128,252 @@ struct CvGeo {
   long long ntiles;
 };
 
+// x = b1 + b2 + b3 for two values, as three packed BF16 pairs (low half = first value)
+__device__ __forceinline__ void split3_bf16(float a, float b, uint32_t& p1, uint32_t& p2, uint32_t& p3) {
+  const __nv_bfloat162 h1 = __floats2bfloat162_rn(a, b);
+  const float2 f1 = __bfloat1622float2(h1);
+  const float ra = a - f1.x, rb = b - f1.y;
+  const __nv_bfloat162 h2 = __floats2bfloat162_rn(ra, rb);
+  const float2 f2 = __bfloat1622float2(h2);
+  const __nv_bfloat162 h3 = __floats2bfloat162_rn(ra - f2.x, rb - f2.y);
+  p1 = *reinterpret_cast<const uint32_t*>(&h1);
+  p2 = *reinterpret_cast<const uint32_t*>(&h2);
+  p3 = *reinterpret_cast<const uint32_t*>(&h3);
+}
+
+// any of the 256 worker threads (warps 0-7, named barrier 1) has v set; all of them get the answer
+__device__ __forceinline__ bool workers_any(bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.or.pred q, 1, 256, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}" : "=r"(r) : "r"((uint32_t)v) : "memory");
+  return r != 0;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar) : "memory");
+}
+
+constexpr int kFwWorkers = 256, kFwThreads = kFwWorkers + 32;   // warps 0-7 workers, warp 8 issues the MMAs
+
 template <int CIN, int COUT>
-__global__ void __launch_bounds__(kCvThreads, 1) conv3d_tc_kernel(const float* __restrict__ x,
+__global__ void __launch_bounds__(kFwThreads, 1) conv3d_tc_kernel(const float* __restrict__ x,
                                                                   const uint16_t* __restrict__ wb,
                                                                   const float* __restrict__ bias,
                                                                   const float* __restrict__ add, float* __restrict__ y,
                                                                   CvGeo G, int relu, int* err) {
   using Lay = CvLayout<CIN, COUT>;
-  constexpr int NP = Lay::NP, HP = Lay::HP, NCH = Lay::NCH;
-  constexpr int ITEMS = 128 * NCH / kCvThreads;                    // 16-byte chunks per thread per tap
-  static_assert(128 * NCH % kCvThreads == 0, "chunk count must divide over the threads");
-  constexpr uint32_t idesc = umma_idesc_tf32(128, NP);
+  constexpr int NP = Lay::NP, KS = Lay::KS, RC = Lay::RC, NPL = Lay::NPL;
+  constexpr uint32_t idesc = umma_idesc_bf16(128, NP);
+  constexpr uint32_t kCols = 2 * NP;                               // two accumulators: 32 or 64 columns
+  static_assert(NPL == 3, "the operand split writes three planes");
+  static_assert(KS <= 4, "mbarrier slots");
   extern __shared__ __align__(1024) unsigned char smem[];
-  unsigned long long* mbar = reinterpret_cast<unsigned long long*>(smem + Lay::off_hdr);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + Lay::off_hdr + 32);
+  // mbarriers: conv_full[s] (workers -> MMA warp: K step s of the planes written), mma_done[s]
+  // (MMA warp -> workers: K step s read), acc_full[a] / acc_empty[a] per accumulator, drain
+  unsigned long long* mb = reinterpret_cast<unsigned long long*>(smem + Lay::off_hdr);
+  unsigned long long* conv_full = mb;
+  unsigned long long* mma_done = mb + 4;
+  unsigned long long* acc_full = mb + 8;
+  unsigned long long* acc_empty = mb + 10;
+  unsigned long long* drain = mb + 12;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + Lay::off_hdr + 128);
+  unsigned char* pl = smem + Lay::off_pl;
   unsigned char* wsm = smem + Lay::off_w;
-  unsigned char* asm_ = smem + Lay::off_a;
-  float* halo = reinterpret_cast<float*>(smem + Lay::off_halo);
+  unsigned char* raw = smem + Lay::off_raw;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(32u));
+                 "r"(kCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
-    for (int b = 0; b < 3; ++b) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[b])));
+    for (int b = 0; b < 13; ++b) {
+      const uint32_t cnt = (b < 4 || b == 10 || b == 11) ? (uint32_t)kFwWorkers : 1u;
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&mb[b])), "r"(cnt));
+    }
     asm volatile("fence.mbarrier_init.release.cluster;");
   }
-  // operand planes and weight blocks start zeroed (K padding CIN..31, N padding COUT..NP-1)
-  for (int i = tid; i < (int)((Lay::off_halo - Lay::off_w) / 16); i += kCvThreads)
-    reinterpret_cast<float4*>(wsm)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+  // weights W[tap][ci][co] (BF16) -> tap block, chunk ci / 8, row co, element ci % 8;
+  // padding rows (co >= COUT) and columns (ci >= CIN) stay zero
+  for (int i = tid; i < 27 * Lay::WT / 16; i += kFwThreads) reinterpret_cast<uint4*>(wsm)[i] = make_uint4(0u, 0u, 0u, 0u);
   __syncthreads();
-  for (int i = tid; i < 27 * CIN * COUT; i += kCvThreads) {   // W[tap][ci][co] -> tap block, row co, column ci
-    const int co = i % COUT, r = i / COUT, ci = r % CIN, tap = r / CIN;
-    *reinterpret_cast<uint32_t*>(wsm + (size_t)tap * NP * 128 + op_offset(co, ci)) = (uint32_t)wb[i] << 16;
+  for (int i = tid; i < 27 * CIN * COUT; i += kFwThreads) {
+    const int tap = i / (CIN * COUT), r = i - tap * (CIN * COUT), ci = r / COUT, co = r - ci * COUT;
+    *reinterpret_cast<uint16_t*>(wsm + tap * Lay::WT + (ci >> 3) * NP * 16 + co * 16 + (ci & 7) * 2) = wb[i];
   }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = *tmem_slot;
-  uint32_t phase[3] = {0u, 0u, 0u};
-  bool used[2] = {false, false};
+  // tile i of this CTA is blockIdx.x + i gridDim.x
+  const long long n = (long long)blockIdx.x < G.ntiles ? (G.ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
   bool failed = false;
-  int gpar = 0;
-  // this thread's operand chunks: row a (tile voxel) and 4-channel chunk c, as halo index and
-  // swizzled plane offset (the same for every tap and tile)
-  int hb[ITEMS], po[ITEMS];
-#pragma unroll
-  for (int j = 0; j < ITEMS; ++j) {
-    const int e = tid + j * kCvThreads;
-    const int a = e / NCH, c = e - a * NCH;
-    const int lx = a & 7, ly = (a >> 3) & 3, lz = a >> 5;
-    hb[j] = (lx + kCvHX * (ly + kCvHY * lz)) * HP + 4 * c;
-    po[j] = (a >> 3) * 1024 + (a & 7) * 128 + (((c ^ a) & 7) << 4);
-  }
 
-  for (long long tile = blockIdx.x; tile < G.ntiles && !failed; tile += gridDim.x) {
-    const int ox = (int)(tile % G.tx) * kCvTX;
-    const long long rt = tile / G.tx;
-    const int oy = (int)(rt % G.ty) * kCvTY, oz = (int)(rt / G.ty) * kCvTZ;
-    for (int i = tid; i < kCvHV * HP; i += kCvThreads) {   // channels CIN..HP-1 are zero padding
-      const int hv = i / HP, c = i - hv * HP;
-      const int hx = hv % kCvHX, hy = (hv / kCvHX) % kCvHY, hz = hv / (kCvHX * kCvHY);
-      const int gx = ox + hx - 1, gy = oy + hy - 1, gz = oz + hz - 1;
-      float v = 0.f;
-      if (c < CIN && gx >= 0 && gx < G.nx && gy >= 0 && gy < G.ny && gz >= 0 && gz < G.nz)
-        v = x[((long long)gx + (long long)G.nx * (gy + (long long)G.ny * gz)) * CIN + c];
-      halo[i] = v;
-    }
-    __syncthreads();
-    for (int tap = 0; tap < 27; ++tap) {
-      const int b = gpar;
-      if (used[b]) {   // the MMAs that read this buffer two taps ago must be done
-        const bool ok = mbar_wait(smem_u32(&mbar[b]), phase[b]);
-        phase[b] ^= 1u;
-        if (__syncthreads_or(!ok)) { failed = true; break; }
+  if (warp < 8) {
+    // FP32 halo of tile t into the staging buffer (4-channel chunk r of halo voxel h at
+    // (r NV + h) 16 bytes), zero outside the volume and for channels >= CIN
+    constexpr int VW = CIN % 4 == 0 ? 4 : 1, PER = 4 * RC / VW;
+    auto load_raw = [&](long long t) {
+      const int hx0 = (int)(t % G.tx) * kFwTX - 1;
+      const long long rt = t / G.tx;
+      const int hy0 = (int)(rt % G.ty) * kFwTY - 1, hz0 = (int)(rt / G.ty) - 1;
+      for (int i = tid; i < kFwNV * PER; i += kFwWorkers) {
+        const int h = i / PER, c = (i - h * PER) * VW;
+        const int hx = h % kFwHX, hy = (h / kFwHX) % kFwHY, hz = h / (kFwHX * kFwHY);
+        const int gx = hx0 + hx, gy = hy0 + hy, gz = hz0 + hz;
+        const bool in = c < CIN && gx >= 0 && gx < G.nx && gy >= 0 && gy < G.ny && gz >= 0 && gz < G.nz;
+        const float* src = in ? x + ((long long)gx + (long long)G.nx * (gy + (long long)G.ny * gz)) * CIN + c : x;
+        const uint32_t dst = smem_u32(raw + ((size_t)(c >> 2) * kFwNV + h) * 16 + (c & 3) * 4);
+        if constexpr (VW == 4)
+          asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(in ? 16 : 0) : "memory");
+        else
+          asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst), "l"(src), "r"(in ? 4 : 0) : "memory");
       }
-      unsigned char* hi = asm_ + (size_t)b * 2 * kCvPlane;
-      unsigned char* lo = hi + kCvPlane;
-      const int dx = tap % 3, dy = (tap / 3) % 3, dz = tap / 9;
-      const int toff = (dx + kCvHX * (dy + kCvHY * dz)) * HP;
+      asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    // K step s of the staging buffer -> the three BF16 planes (item = 8 channels of one voxel)
+    auto convert = [&](int s) {
+      for (int i = tid; i < 2 * kFwNV; i += kFwWorkers) {
+        const int c = 2 * s + (i >= kFwNV ? 1 : 0), h = i - (i >= kFwNV ? kFwNV : 0);
+        const float4 v0 = *reinterpret_cast<const float4*>(raw + ((size_t)(2 * c) * kFwNV + h) * 16);
+        const float4 v1 = *reinterpret_cast<const float4*>(raw + ((size_t)(2 * c + 1) * kFwNV + h) * 16);
+        uint4 q1, q2, q3;
+        split3_bf16(v0.x, v0.y, q1.x, q2.x, q3.x);
+        split3_bf16(v0.z, v0.w, q1.y, q2.y, q3.y);
+        split3_bf16(v1.x, v1.y, q1.z, q2.z, q3.z);
+        split3_bf16(v1.z, v1.w, q1.w, q2.w, q3.w);
+        unsigned char* o = pl + (size_t)c * kFwCS + (size_t)h * 16;
+        *reinterpret_cast<uint4*>(o) = q1;
+        *reinterpret_cast<uint4*>(o + Lay::PB) = q2;
+        *reinterpret_cast<uint4*>(o + 2 * Lay::PB) = q3;
+      }
+    };
+    // accumulator of tile j -> y: warp w reads TMEM lanes 32 (w & 3) .. + 31 (tile rows) and
+    // the column half w >> 2; returns false when the wait for the MMAs ran out
+    constexpr int HC = NP / 2;
+    const int q = warp & 3, hs = warp >> 2;
+    float bz[HC];
 #pragma unroll
-      for (int j = 0; j < ITEMS; ++j) {
-        const float4 v = *reinterpret_cast<const float4*>(halo + hb[j] + toff);
-        uint4 h;
-        h.x = tf32_rna(v.x); h.y = tf32_rna(v.y); h.z = tf32_rna(v.z); h.w = tf32_rna(v.w);
-        const float4 l = make_float4(v.x - __uint_as_float(h.x), v.y - __uint_as_float(h.y), v.z - __uint_as_float(h.z),
-                                     v.w - __uint_as_float(h.w));
-        *reinterpret_cast<uint4*>(hi + po[j]) = h;
-        *reinterpret_cast<float4*>(lo + po[j]) = l;
-      }
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      __syncthreads();
-      if (tid == 0) {
-        asm volatile("tcgen05.fence::after_thread_sync;");
-        const uint32_t ah = smem_u32(hi), al = smem_u32(lo);
-        const uint32_t wt = smem_u32(wsm + (size_t)tap * NP * 128);
-#pragma unroll
-        for (int s = 0; s < 4; ++s) {
-          const uint64_t dw = umma_desc_sw128(wt + s * 32);
-          umma_tf32(tmem, umma_desc_sw128(ah + s * 32), dw, idesc, (tap > 0 || s > 0) ? 1u : 0u);
-          umma_tf32(tmem, umma_desc_sw128(al + s * 32), dw, idesc, 1u);
-        }
-        umma_commit(smem_u32(&mbar[b]));
-        if (tap == 26) umma_commit(smem_u32(&mbar[2]));
-      }
-      used[b] = true;
-      gpar ^= 1;
-    }
-    if (failed) break;
-    {
-      const bool ok = mbar_wait(smem_u32(&mbar[2]), phase[2]);
-      phase[2] ^= 1u;
-      for (int bb = 0; bb < 2; ++bb)
-        if (used[bb]) {
-          mbar_wait(smem_u32(&mbar[bb]), phase[bb]);
-          phase[bb] ^= 1u;
-          used[bb] = false;
-        }
-      if (__syncthreads_or(!ok)) { failed = true; break; }
-    }
-    asm volatile("tcgen05.fence::after_thread_sync;");
-    if (warp < 4) {   // warp w holds TMEM lanes 32 w .. 32 w + 31 = tile rows (voxels)
-      uint32_t r[NP];
-      const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16);
-      if constexpr (NP == 32) {
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-            "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-              "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]),
-              "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]),
-              "=r"(r[30]), "=r"(r[31])
-            : "r"(taddr));
-      } else {
+    for (int j = 0; j < HC; ++j) bz[j] = (bias && hs * HC + j < COUT) ? bias[hs * HC + j] : 0.f;
+    auto epilogue = [&](long long j) -> bool {
+      const uint32_t acc = (uint32_t)(j & 1);
+      const bool ok = mbar_wait(smem_u32(&acc_full[acc]), (uint32_t)((j >> 1) & 1));
+      if (workers_any(!ok)) return false;
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      uint32_t r[HC];
+      const uint32_t taddr = tmem + ((uint32_t)(32 * q) << 16) + acc * NP + hs * HC;
+      if constexpr (HC == 16) {
         asm volatile(
             "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
             : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
               "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
             : "r"(taddr));
+      } else {
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                     : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                     : "r"(taddr));
       }
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      const int a = 32 * warp + lane;
-      const int gx = ox + (a & 7), gy = oy + ((a >> 3) & 3), gz = oz + (a >> 5);
-      if (gx < G.nx && gy < G.ny && gz < G.nz) {
+      asm volatile("tcgen05.fence::before_thread_sync;");
+      mbar_arrive(smem_u32(&acc_empty[acc]));   // the MMA warp may reuse this accumulator
+      const long long t = (long long)blockIdx.x + j * gridDim.x;
+      const int a = 32 * q + lane;
+      const int gx = (int)(t % G.tx) * kFwTX + (a & 7);
+      const long long rt = t / G.tx;
+      const int gy = (int)(rt % G.ty) * kFwTY + (a >> 3), gz = (int)(rt / G.ty);
+      if (gx < G.nx && gy < G.ny) {
         const long long v = (long long)gx + (long long)G.nx * (gy + (long long)G.ny * gz);
+        float o[HC];
 #pragma unroll
-        for (int c = 0; c < COUT; ++c) {
-          float val = __uint_as_float(r[c]) + (bias ? bias[c] : 0.f);
+        for (int k = 0; k < HC; ++k) {
+          float val = __uint_as_float(r[k]) + bz[k];
           if (relu) val = fmaxf(val, 0.f);
-          if (add) val += add[v * COUT + c];
-          y[v * COUT + c] = val;
+          o[k] = val;
+        }
+        if constexpr (COUT == 2 * HC && HC % 4 == 0) {   // whole 16-byte groups of this voxel's channels
+          float4* yp = reinterpret_cast<float4*>(y + v * COUT + hs * HC);
+          const float4* ap = add ? reinterpret_cast<const float4*>(add + v * COUT + hs * HC) : nullptr;
+#pragma unroll
+          for (int k = 0; k < HC / 4; ++k) {
+            float4 w4 = make_float4(o[4 * k], o[4 * k + 1], o[4 * k + 2], o[4 * k + 3]);
+            if (ap) {
+              const float4 a4 = ap[k];
+              w4.x += a4.x; w4.y += a4.y; w4.z += a4.z; w4.w += a4.w;
+            }
+            yp[k] = w4;
+          }
+        } else {
+#pragma unroll
+          for (int k = 0; k < HC; ++k) {
+            const int c = hs * HC + k;
+            if (c < COUT) y[v * COUT + c] = o[k] + (add ? add[v * COUT + c] : 0.f);
+          }
         }
       }
+      return true;
+    };
+
+    if (n > 0) load_raw(blockIdx.x);
+    for (long long i = 0; i < n && !failed; ++i) {
+      asm volatile("cp.async.wait_all;" ::: "memory");
+      asm volatile("bar.sync 1, 256;" ::: "memory");
+      for (int s = 0; s < KS; ++s) {
+        if (i > 0) {   // the MMAs of tile i - 1 no longer read K step s of the planes
+          const bool ok = mbar_wait(smem_u32(&mma_done[s]), (uint32_t)((i - 1) & 1));
+          if (workers_any(!ok)) { failed = true; break; }
+        }
+        convert(s);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_arrive(smem_u32(&conv_full[s]));
+      }
+      if (failed) break;
+      asm volatile("bar.sync 1, 256;" ::: "memory");   // every worker is done with the staging buffer
+      if (i + 1 < n) load_raw((long long)blockIdx.x + (i + 1) * gridDim.x);
+      if (i > 0 && !epilogue(i - 1)) failed = true;
     }
-    asm volatile("tcgen05.fence::before_thread_sync;");
-    __syncthreads();
+    if (!failed && n > 0 && !epilogue(n - 1)) failed = true;
+    asm volatile("cp.async.wait_all;" ::: "memory");
+  } else if (lane == 0) {
+    const uint64_t a0 = umma_desc_kmajor(smem_u32(pl), kFwCS, kFwHX * 16);
+    const uint64_t b0 = umma_desc_kmajor(smem_u32(wsm), NP * 16, 128);
+    for (long long i = 0; i < n && !failed; ++i) {
+      const uint32_t acc = (uint32_t)(i & 1);
+      if (i >= 2 && !mbar_wait(smem_u32(&acc_empty[acc]), (uint32_t)(((i - 2) >> 1) & 1))) { failed = true; break; }
+      const uint32_t d = tmem + acc * NP;
+      for (int s = 0; s < KS; ++s) {
+        if (!mbar_wait(smem_u32(&conv_full[s]), (uint32_t)(i & 1))) { failed = true; break; }
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        // descriptor start addresses advance in 16-byte units
+        const uint64_t as = a0 + (uint64_t)((s * 2 * kFwCS) >> 4), bs = b0 + (uint64_t)((s * 2 * NP * 16) >> 4);
+#pragma unroll 1
+        for (int dzy = 0; dzy < 9; ++dzy) {   // dy + 3 dz
+          const uint32_t vrow = (uint32_t)(kFwHX * (dzy % 3 + kFwHY * (dzy / 3)));
+#pragma unroll
+          for (int dx = 0; dx < 3; ++dx) {
+            const uint64_t db = bs + (uint64_t)(((3 * dzy + dx) * Lay::WT) >> 4);
+#pragma unroll
+            for (int p = 0; p < NPL; ++p) {
+              const uint64_t da = as + (uint64_t)((p * Lay::PB) >> 4) + vrow + dx;
+              umma_bf16(d, da, db, idesc, (s > 0 || dzy > 0 || dx > 0 || p > 0) ? 1u : 0u);
+            }
+          }
+        }
+        umma_commit(smem_u32(&mma_done[s]));
+      }
+      if (failed) break;
+      umma_commit(smem_u32(&acc_full[acc]));
+    }
   }
-  if (failed && tid == 0 && err) atomicExch(err, 1);
-  // nothing may still write the accumulator when it is released
-  if (tid == 0) umma_commit(smem_u32(&mbar[2]));
-  mbar_wait(smem_u32(&mbar[2]), phase[2]);
+  if (failed && err) atomicExch(err, 1);
+  __syncthreads();
+  // nothing may still write an accumulator when tensor memory is released
+  if (warp == 8 && lane == 0) umma_commit(smem_u32(drain));
+  mbar_wait(smem_u32(drain), 0u);
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(32u));
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols));
 }
 
 // ---------------------------------------------------------------------------------------
@@ -605,6 +712,8 @@ int conv_inst(const float* x, const uint16_t* w, const float* b, const float* ad
               int* err, cudaStream_t s) {
   const size_t smem = CvLayout<CIN, COUT>::total;
   static_assert(CvLayout<CIN, COUT>::total <= 227 * 1024, "conv operands exceed shared memory");
+  if (CIN % 4 == 0 && (reinterpret_cast<uintptr_t>(x) & 15) != 0)
+    return set_error(LLR_ERR_INVALID, "conv3d input must be 16-byte aligned for %d channels", CIN);
   auto k = conv3d_tc_kernel<CIN, COUT>;
   LLR_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int dev = 0, nsm = 0;
@@ -612,12 +721,12 @@ int conv_inst(const float* x, const uint16_t* w, const float* b, const float* ad
   LLR_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   CvGeo G;
   G.nx = dims[0]; G.ny = dims[1]; G.nz = dims[2];
-  G.tx = (G.nx + kCvTX - 1) / kCvTX;
-  G.ty = (G.ny + kCvTY - 1) / kCvTY;
-  G.ntiles = (long long)G.tx * G.ty * ((G.nz + kCvTZ - 1) / kCvTZ);
+  G.tx = (G.nx + kFwTX - 1) / kFwTX;
+  G.ty = (G.ny + kFwTY - 1) / kFwTY;
+  G.ntiles = (long long)G.tx * G.ty * G.nz;
   const long long grid = std::min<long long>(G.ntiles, nsm);
   note_launch();
-  k<<<(unsigned)grid, kCvThreads, smem, s>>>(x, w, b, add, y, G, relu, err);
+  k<<<(unsigned)grid, kFwThreads, smem, s>>>(x, w, b, add, y, G, relu, err);
   LLR_CUDA_TRY(cudaGetLastError());
   return LLR_OK;
 }

@@ -1,6 +1,7 @@
 // Shared helpers for the kernels that drive the 5th-generation tensor cores (tcgen05):
-// UMMA shared-memory and instruction descriptors, the TF32 MMA, commits to mbarriers, bounded
-// mbarrier waits, the TF32 split and the 128-byte swizzled K-major operand layout.
+// UMMA shared-memory and instruction descriptors (128-byte swizzled and unswizzled K-major), the
+// TF32 and BF16 MMAs, commits to mbarriers, bounded mbarrier waits, the TF32 split and the
+// 128-byte swizzled operand layout.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -22,6 +23,30 @@ __device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
   d |= (uint64_t)1 << 46;
   d |= (uint64_t)2 << 61;                          // SWIZZLE_128B
   return d;
+}
+
+// K-major UMMA shared-memory descriptor without swizzle: core matrices of 8 rows x 16 B stored
+// as 128 contiguous bytes (row stride 16 B); lbo = byte step between core matrices along K,
+// sbo = byte step between 8-row groups along M / N.  The start address needs 16-byte alignment
+// only, so an operand can begin at any 16-byte row of a larger array.
+__device__ __forceinline__ uint64_t umma_desc_kmajor(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;                          // SWIZZLE_NONE (layout type 0)
+  return d;
+}
+
+// Instruction descriptor: BF16 x BF16 -> F32, both operands K-major, M x N.
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(uint32_t M, uint32_t N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((N >> 3) << 17) | ((M >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
 }
 
 // Instruction descriptor: TF32 x TF32 -> F32, both operands K-major, M x N.
