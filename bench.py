@@ -341,10 +341,10 @@ def run_b200(args, dist: Dist) -> None:
     hist = ctx.residual_history(args.steps)
     value = dist.world * args.steps / (t_max / 1e3)
 
-    # roofline of the dominant stage: the LLR proximal step, two kernels per iteration
-    # (llr_gram_tc_kernel: gather + 3xTF32 tcgen05 Gram; llr_eig_apply_kernel: eigen
-    # decomposition + apply + scatter). Algorithmic bytes = the operator's minimum, one read and
-    # one write of every complex64 element of the iterate (16 B per voxel-volume element).
+    # roofline of the dominant stage: the LLR proximal step (llr_gram_tc_kernel: gather + 3xTF32
+    # tcgen05 Gram; llr_eig_warp_kernel: eigen decomposition; llr_apply_kernel: apply + scatter).
+    # Algorithmic bytes = the operator's minimum, one read and one write of every complex64
+    # element of the iterate (16 B per voxel-volume element).
     names = ["llr_prox", "wavelet", "fft_fwd", "dc", "fft_inv"]
     per_launch_ms = {n: stage_ms[i] / args.steps for i, n in enumerate(names)}
     prox_bytes = 16.0 * E
@@ -526,7 +526,7 @@ def main(argv=None):
     ap.add_argument("--fft-mode", type=int, default=0,
                     help="0: fused per-plane FFT + DC + inverse FFT kernel; 1: cuFFT passes")
     ap.add_argument("--eig-solver", type=int, default=0,
-                    help="0: tridiagonal, warp per block; 1: Jacobi; 2: tridiagonal, CTA per block")
+                    help="0: tridiagonal, warp per block; 1: Jacobi")
     ap.add_argument("--ncu-traffic", metavar="CSV",
                     help="write profiles/<--traffic-name>_<--config>.json from `ncu -i REP --page raw --csv` output "
                          "and exit")

@@ -66,8 +66,7 @@ typedef struct llr_config {
   int32_t n_iter;             /* default iteration count (lib.rs:62)                 */
   uint64_t seed;              /* key of the counter-based shift RNG                  */
   int32_t device;             /* CUDA device ordinal                                 */
-  int32_t eig_solver;         /* 0: tridiagonal, warp per block (default); 1: Jacobi;
-                                  2: tridiagonal, CTA per block                          */
+  int32_t eig_solver;         /* 0: tridiagonal, warp per block (default); 1: Jacobi  */
   int32_t gram_mode;          /* 0: 3xTF32 tensor cores (default); 1: FP32 FMA        */
   int32_t fft_mode;           /* 0: fused FFT + DC + inverse FFT per (x, volume) plane
                                   where the plane fits (default); 1: cuFFT passes       */
@@ -158,6 +157,13 @@ int llr_get_iteration(const llr_ctx* ctx, int64_t* it);
 int llr_set_iteration(llr_ctx* ctx, int64_t it);
 /* Residual history of the last `count` iterations ending at the current one. */
 int llr_get_residual_history(llr_ctx* ctx, double* out, int32_t count);
+/* Objective history, same window: F(x) = 0.5 ||M A x - y||^2 + lambda sum_b ||X_b||_* of each
+ * iteration's prox output x (FP64 sums; the nuclear norms from the prox's own singular values).
+ * Defined for the soft threshold on one non-overlapping tiling with no wavelet or subspace term
+ * (hard rank: the data term alone); NaN otherwise.  With a fixed block partition it is the
+ * function the proximal-gradient iteration (step 1, unitary A) decreases monotonically.  No
+ * reference counterpart (lib.rs:321-325 records only the residual). */
+int llr_get_objective_history(llr_ctx* ctx, double* out, int32_t count);
 /* sum |y|^2 and numel/nnz of the measurements (lib.rs:409-417). */
 int llr_measurement_stats(llr_ctx* ctx, double* total_energy, double* undersampling);
 /* Largest block singular value of the current iterate at `shift` (FP32 Gram + Jacobi). */

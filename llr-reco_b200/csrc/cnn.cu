@@ -1,8 +1,9 @@
 // Learned warm start: a small 3-D residual CNN (conv3d 3x3x3, zero padding, ReLU between
 // layers, out = in + net(in)) with hand-written forward, backward-data and backward-weight
 // kernels, mean-squared-error loss and Adam.  BF16 weights feed the convolutions with FP32
-// accumulation (forward and backward-data on the tensor cores, tcgen05 TF32 with the
-// activations split hi + lo); the optimizer keeps FP32 master weights.
+// accumulation on the tensor cores: forward and backward-data as tcgen05 kind::f16 MMAs with
+// the activations split into three BF16 planes, the weight gradient as 3xTF32 MMAs; the
+// optimizer keeps FP32 master weights.
 //
 // Activations are channels-last FP32, voxel v = x + nx (y + ny z) (the reference image order,
 // x fastest).  Forward:  y[v][co] = b[co] + sum_{tap, ci} W[tap][ci][co] x[v + d(tap) - 1][ci],

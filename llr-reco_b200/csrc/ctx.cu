@@ -20,6 +20,8 @@ int launch_dc_hybrid(float2* u, const float2* yhat, const int* pos, const long l
                      double* partials, int n_part_x, int replace_only, cudaStream_t s);
 int launch_dc_full(float2* u, const float2* yhat, long long n, double* partials, int nblocks, int replace_only,
                    cudaStream_t s);
+int launch_objective(const double* blk_nuc, long long nb, double lam, const double* hist, double* obj, long long cap,
+                     const long long* it, cudaStream_t s);
 int launch_finalize(const double* partials, int np, double scale, double* hist, long long cap, long long* it,
                     int advance, double* out, cudaStream_t s);
 int launch_line_nnz(const float2* y, long long nlines, int nx, int* cnt, cudaStream_t s);
@@ -227,6 +229,10 @@ static int prox_pass(llr_ctx* c, cudaStream_t s, const int* explicit_shift, bool
     op.defer_zero = (!standalone && !block_stat && !explicit_shift && defer_zero_blocks(c)) ? 1 : 0;
     op.vwide = c->d_vwide;
     op.vwide_ctas = c->vwide_ctas;
+    if (c->obj_mode == 2 && !standalone && !block_stat && !explicit_shift) {
+      LLR_CUDA_TRY(cudaMemsetAsync(c->d_blk_nuc, 0, sizeof(double) * (size_t)std::max<long long>(1, c->nblocks), s));
+      op.blk_nuc = c->d_blk_nuc;
+    }
     if (!c->phase_off.empty() && !block_stat) {
       // overlapping blocks: every phase of the strided grid is a non-overlapping tiling at the
       // shift plus the phase offset; the mean of the phases goes to d_work, then back to d_x
@@ -291,14 +297,23 @@ static int dc_pass(llr_ctx* c, cudaStream_t s, int replace_only) {
 
 static int n_partials(const llr_ctx* c) { return c->hybrid ? kPartX * c->g.nq : kPartFull; }
 
+// Residual of iteration k from the DC partials into the history (advancing the counter), then
+// the objective of the prox output of the same iteration.
+static int finalize_iteration(llr_ctx* c, int np, cudaStream_t s) {
+  LLR_TRY(launch_finalize(c->d_partials, np, (double)c->load_scale, c->d_hist, c->hist_cap, c->d_iter, 1, nullptr, s));
+  if (c->obj_mode == 0) return LLR_OK;
+  return launch_objective(c->obj_mode == 2 ? c->d_blk_nuc : nullptr, std::max<long long>(1, c->nblocks),
+                          (double)c->cfg.lambda, c->d_hist, c->d_obj, c->hist_cap, c->d_iter, s);
+}
+
 // Forward 2-D DFT, DC with residual, inverse 2-D DFT in one kernel; residual finalized.
 static int fused_dc_pass(llr_ctx* c, cudaStream_t s, double* out) {
   const bool zf = defer_zero_blocks(c);
   const BlockSource zsrc = make_source(c, nullptr, 1.f);
   LLR_TRY(launch_fft_dc(c->d_x, c->d_yhat, c->d_samp_pos, c->d_samp_off, c->d_fft_tw, c->g, c->d_partials,
                         c->fft_grid, zf ? c->d_blk_ra : nullptr, zf ? &zsrc : nullptr, s));
-  return launch_finalize(c->d_partials, c->fft_grid, (double)c->load_scale, out ? nullptr : c->d_hist,
-                         out ? 0 : c->hist_cap, out ? nullptr : c->d_iter, out ? 0 : 1, out, s);
+  if (!out) return finalize_iteration(c, c->fft_grid, s);
+  return launch_finalize(c->d_partials, c->fft_grid, (double)c->load_scale, nullptr, 0, nullptr, 0, out, s);
 }
 
 int ctx_enqueue_iteration(llr_ctx* c, cudaStream_t s) {
@@ -307,8 +322,7 @@ int ctx_enqueue_iteration(llr_ctx* c, cudaStream_t s) {
   if (c->fused_fft) return fused_dc_pass(c, s, nullptr);
   LLR_TRY(exec_fft(c, c->d_x, CUFFT_FORWARD, s));
   LLR_TRY(dc_pass(c, s, 0));
-  LLR_TRY(launch_finalize(c->d_partials, n_partials(c), (double)c->load_scale, c->d_hist, c->hist_cap, c->d_iter, 1,
-                          nullptr, s));
+  LLR_TRY(finalize_iteration(c, n_partials(c), s));
   LLR_TRY(exec_fft(c, c->d_x, CUFFT_INVERSE, s));
   return LLR_OK;
 }
@@ -361,6 +375,8 @@ int llr_ctx_create(const llr_config* cfg, llr_ctx** out) {
   if ((st = dalloc(&c->d_partials, (size_t)c->n_partials))) return fail(st);
   c->hist_cap = kHistCap;
   if ((st = dalloc(&c->d_hist, (size_t)c->hist_cap))) return fail(st);
+  if ((st = dalloc(&c->d_obj, (size_t)c->hist_cap))) return fail(st);
+  if ((st = dalloc(&c->d_blk_nuc, (size_t)std::max<long long>(1, c->nblocks)))) return fail(st);
   if ((st = dalloc(&c->d_iter, 1))) return fail(st);
   if ((st = dalloc(&c->d_block_stat, (size_t)std::max<long long>(1, c->nblocks)))) return fail(st);
   if ((st = dalloc(&c->d_fb, (size_t)std::max<long long>(1, c->nblocks) + 1))) return fail(st);
@@ -393,6 +409,7 @@ int llr_ctx_create(const llr_config* cfg, llr_ctx** out) {
     return fail(st);
   e = cudaMemsetAsync(c->d_iter, 0, sizeof(long long), c->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(c->d_hist, 0, sizeof(double) * c->hist_cap, c->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->d_obj, 0xFF, sizeof(double) * c->hist_cap, c->stream);   // NaN
   if (e == cudaSuccess) e = cudaMemsetAsync(c->d_x, 0, sizeof(float2) * E, c->stream);
   if (e != cudaSuccess) return fail(cuda_error(e, "cudaMemsetAsync", __FILE__, __LINE__));
   if (cfg->subspace_rank > 0 && (st = dalloc(&c->d_S, (size_t)c->g.nq * cfg->subspace_rank))) return fail(st);
@@ -419,6 +436,12 @@ int llr_ctx_create(const llr_config* cfg, llr_ctx** out) {
       c->wavelet_on = true;
     }
   }
+  // The objective 0.5 ||M A x - y||^2 + lambda sum_b ||X_b||_* is the function the iteration
+  // minimises when the prox is the exact soft threshold of one tiling and nothing else acts on
+  // the iterate; hard rank keeps the data term (the rank constraint holds by construction).
+  // Overlapping tilings, wavelets and the subspace model have no such single objective here.
+  const bool plain = cfg->subspace_rank == 0 && !c->wavelet_on && c->phase_off.empty();
+  c->obj_mode = !plain ? 0 : (cfg->prox_mode == LLR_PROX_SOFT_THRESH ? 2 : 1);
   if ((st = upload_tables(c))) return fail(st);
   c->h_iter = 0;
   *out = c;
@@ -433,6 +456,7 @@ int llr_ctx_destroy(llr_ctx* c) {
   if (c->have_plan) cufftDestroy(c->plan_fwd);
   dfree(c->d_x); dfree(c->d_work); dfree(c->d_yhat); dfree(c->d_samp_pos); dfree(c->d_samp_off);
   dfree(c->d_ph_ksp); dfree(c->d_ph_img); dfree(c->d_S); dfree(c->d_partials); dfree(c->d_hist); dfree(c->d_iter);
+  dfree(c->d_obj); dfree(c->d_blk_nuc);
   dfree(c->d_block_stat); dfree(c->d_fb); dfree(c->d_gram); dfree(c->d_blk_ra); dfree(c->d_fft_tw); dfree(c->d_err); dfree(c->d_vwide); dfree(c->d_wavelet_work); dfree(c->d_fft_work);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -681,9 +705,7 @@ static int capture_stage(llr_ctx* c, int stage, cudaGraphExec_t* out) {
     case 3:
       if (c->fused_fft) break;
       st = dc_pass(c, s, 0);
-      if (st == LLR_OK)
-        st = launch_finalize(c->d_partials, n_partials(c), (double)c->load_scale, c->d_hist, c->hist_cap, c->d_iter,
-                             1, nullptr, s);
+      if (st == LLR_OK) st = finalize_iteration(c, n_partials(c), s);
       break;
     case 4: if (!c->fused_fft) st = exec_fft(c, c->d_x, CUFFT_INVERSE, s); break;
   }
@@ -888,6 +910,20 @@ int llr_get_residual_history(llr_ctx* c, double* out, int32_t count) {
   const long long nn = hi - lo;
   if (nn > 0)
     LLR_CUDA_TRY(cudaMemcpyAsync(out + (count - nn), c->d_hist + lo, sizeof(double) * nn, cudaMemcpyDeviceToHost,
+                                 c->stream));
+  LLR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return LLR_OK;
+}
+
+int llr_get_objective_history(llr_ctx* c, double* out, int32_t count) {
+  if (!c || !out || count < 0) return set_error(LLR_ERR_INVALID, "bad arguments");
+  LLR_CUDA_TRY(cudaSetDevice(c->device));
+  const long long hi = std::min<long long>(c->h_iter, c->hist_cap);
+  const long long lo = std::max<long long>(0, hi - count);
+  for (int i = 0; i < count; ++i) out[i] = NAN;
+  const long long nn = hi - lo;
+  if (nn > 0 && c->obj_mode != 0)
+    LLR_CUDA_TRY(cudaMemcpyAsync(out + (count - nn), c->d_obj + lo, sizeof(double) * nn, cudaMemcpyDeviceToHost,
                                  c->stream));
   LLR_CUDA_TRY(cudaStreamSynchronize(c->stream));
   return LLR_OK;

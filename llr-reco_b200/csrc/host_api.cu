@@ -189,7 +189,7 @@ int llr_config_validate(const llr_config* c) {
   if (c->subspace_rank > 0 && c->prox_mode == LLR_PROX_HARD_RANK && c->rank > c->subspace_rank)
     return set_error(LLR_ERR_INVALID, "llr rank must be <= subspace rank (lib.rs:217)");
   if (!(c->wavelet_alpha >= 0.f)) return set_error(LLR_ERR_INVALID, "wavelet_alpha must be >= 0");
-  if (c->eig_solver < 0 || c->eig_solver > 2) return set_error(LLR_ERR_INVALID, "eig_solver must be 0, 1 or 2");
+  if (c->eig_solver < 0 || c->eig_solver > 1) return set_error(LLR_ERR_INVALID, "eig_solver must be 0 or 1");
   if (c->gram_mode != 0 && c->gram_mode != 1) return set_error(LLR_ERR_INVALID, "gram_mode must be 0 or 1");
   if (c->fft_mode != 0 && c->fft_mode != 1) return set_error(LLR_ERR_INVALID, "fft_mode must be 0 or 1");
   if (c->wavelet_alpha > 0.f && (c->wavelet_moments < 1 || c->wavelet_moments > 10))

@@ -42,7 +42,7 @@ struct ProxOp {
   int rank;
   float lambda;
   float* block_stat;   // when non-null: write the largest Gram eigenvalue, skip the update
-  int eig_solver;      // 0: tridiagonal, one warp per block; 1: Jacobi; 2: tridiagonal, one CTA per block
+  int eig_solver;      // 0: tridiagonal, one warp per block; 1: Jacobi
   int* fb_list;        // blocks handed to the Jacobi kernel (capacity nblocks)
   int* fb_count;
   float2* gram;        // optional scratch, nblocks * gram_stride: selects the split Gram/eigen path
@@ -54,6 +54,9 @@ struct ProxOp {
                        // FFT that follows in the same iteration zero-fills them as it loads
   float2* vwide = nullptr;  // 64 < n <= 128: per-CTA eigenvector scratch of the wide Jacobi kernel,
   int vwide_ctas = 0;       // vwide_ctas * wide_v_stride() float2
+  double* blk_nuc = nullptr;   // soft threshold: per block sum over its singular values s of
+                               // (s - lambda)+ in FP64, the nuclear norm of the block's prox output
+                               // (the regulariser term of the objective); blocks left at 0 keep none
 };
 
 // Widest Casorati column count of the prox kernels, and the per-CTA eigenvector scratch the
@@ -164,6 +167,9 @@ struct llr_ctx {
   int n_partials;
   double* d_hist;
   long long hist_cap;
+  double* d_obj;            // objective per iteration (FP64; NaN where the model has none)
+  double* d_blk_nuc;        // per-block nuclear-norm terms of the current iteration's prox
+  int obj_mode;             // 0: no objective, 1: data term only (hard rank), 2: data + lambda nuclear
   long long* d_iter;
   long long h_iter;         // host mirror (valid after sync)
   float* d_block_stat;

@@ -88,6 +88,8 @@ __global__ void __launch_bounds__(kLlrThreads) llr_prox_jacobi_kernel(BlockSourc
       continue;
     }
     singular_map(A, lda, n, op.mode, op.rank, op.lambda, ev, g, act, misc);
+    if (op.blk_nuc && op.mode != LLR_PROX_HARD_RANK && threadIdx.x == 0)
+      op.blk_nuc[blk] = nuclear_from_eigs(ev, n, op.lambda);
     const int na = misc->n_active;
     if (!(na == n && op.mode == LLR_PROX_HARD_RANK)) {
       form_W(A, V, lda, n, g, act, na);

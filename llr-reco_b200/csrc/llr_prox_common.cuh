@@ -319,6 +319,17 @@ __device__ void singular_map(const float2* A, int lda, int n, int mode, int rank
   __syncthreads();
 }
 
+// Nuclear norm of a soft-thresholded block from the eigenvalues e of its Gram matrix (squared
+// singular values): sum of (sqrt(e) - lambda)+ in FP64, in index order.
+__device__ __forceinline__ double nuclear_from_eigs(const float* e, int k, float lam) {
+  double t = 0.0;
+  for (int j = 0; j < k; ++j) {
+    const double sv = sqrt((double)fmaxf(e[j], 0.f));
+    if (sv > (double)lam) t += sv - (double)lam;
+  }
+  return t;
+}
+
 // W = V diag(g) V^H written into A (lda).
 __device__ void form_W(float2* A, const float2* V, int lda, int n, const float* g, const int* act, int na) {
   for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {

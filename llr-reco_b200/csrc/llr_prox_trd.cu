@@ -750,6 +750,8 @@ __global__ void __launch_bounds__(kLlrThreads, 2) llr_prox_trd_kernel(BlockSourc
       }
       g[tid] = gv;
     }
+    if (op.blk_nuc && op.mode != LLR_PROX_HARD_RANK && tid == 0)
+      op.blk_nuc[blk] = nuclear_from_eigs(trd->lam, ra, op.lambda);
     __syncthreads();
     if (ra <= 4) apply_rows<4>(src, base, rows, rowph, m, n, qstride, Va, g, ra);
     else if (ra <= 8) apply_rows<8>(src, base, rows, rowph, m, n, qstride, Va, g, ra);
@@ -780,10 +782,10 @@ int launch_trd_instance(const BlockSource& src, const ProxOp& op, cudaStream_t s
 }
 
 // =======================================================================================
-// Split path.  llr_gram_kernel writes every block's Gram matrix (packed lower triangle,
-// n(n+1)/2 complex) to a scratch buffer; llr_eig_apply_kernel (128 threads, several CTAs per
-// SM so that several blocks' serial eigen phases overlap) reads it back into shared memory,
-// runs the tridiagonal eigen path and applies C' = (C V_a) g V_a^H from global to global.
+// Split path.  A Gram kernel (llr_gram_tc_kernel on the tensor cores, or llr_gram_kernel in
+// FP32 FMA) writes every block's Gram matrix (packed lower triangle, n(n+1)/2 complex) to a
+// scratch buffer; the warp eigen kernel turns it into the kept eigenvectors and the apply
+// kernel forms C' = (C V_a) g V_a^H from global to global.
 // =======================================================================================
 template <int NPMAX, int TG>
 __global__ void __launch_bounds__(kLlrThreads, 2) llr_gram_kernel(BlockSource src, ProxOp op, TrdLayout L) {
@@ -806,150 +808,13 @@ __global__ void __launch_bounds__(kLlrThreads, 2) llr_gram_kernel(BlockSource sr
   }
 }
 
-constexpr int kEigThreads = 128;
-
-struct EigLayout {
-  size_t off_row, off_rowph, off_A, off_trd, off_V, off_g, off_work, total;
-};
-
-template <int NPMAX>
-EigLayout make_eig_layout(int m) {
-  EigLayout L;
-  size_t off = 256;
-  L.off_row = off; off = align16(off + sizeof(RowTab) * (size_t)m);
-  L.off_rowph = off; off = align16(off + sizeof(float2) * (size_t)m);
-  L.off_A = off; off = align16(off + sizeof(float2) * (size_t)NPMAX * (NPMAX + 1) / 2);
-  L.off_trd = off; off = align16(off + sizeof(TrdSmem<NPMAX>));
-  L.off_V = off; off = align16(off + sizeof(float2) * NPMAX * kRaMax);
-  L.off_g = off; off = align16(off + sizeof(float) * kRaMax);
-  L.off_work = off; off = align16(off + sizeof(float) * 2 * NPMAX * kRaMax);
-  L.total = off;
-  return L;
-}
-
-template <int NPMAX>
-__global__ void __launch_bounds__(kEigThreads, 4) llr_eig_apply_kernel(BlockSource src, ProxOp op, EigLayout L) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  Misc* misc = reinterpret_cast<Misc*>(smem);
-  RowTab* rows = reinterpret_cast<RowTab*>(smem + L.off_row);
-  float2* rowph = reinterpret_cast<float2*>(smem + L.off_rowph);
-  float2* A = reinterpret_cast<float2*>(smem + L.off_A);
-  TrdSmem<NPMAX>* trd = reinterpret_cast<TrdSmem<NPMAX>*>(smem + L.off_trd);
-  float2* Va = reinterpret_cast<float2*>(smem + L.off_V);
-  float* g = reinterpret_cast<float*>(smem + L.off_g);
-  float* work = reinterpret_cast<float*>(smem + L.off_work);
-  const int m = op.m, n = op.n, tid = threadIdx.x;
-  const long long qstride = src.kind == 1 ? src.g.V : (long long)m;
-  const int P = n * (n + 1) / 2;
-  if (tid == 0) block_shift(src, misc->shift);
-  __syncthreads();
-  const int sh[3] = {misc->shift[0], misc->shift[1], misc->shift[2]};
-
-  for (long long blk = blockIdx.x; blk < src.nblocks; blk += gridDim.x) {
-    const long long base = src.kind == 1 ? 0 : blk * (long long)m * n;
-    const float2* G = op.gram + blk * op.gram_stride;
-    float fro = 0.f;   // ||G||_F^2 from the packed lower triangle
-    for (int i = tid; i < P; i += blockDim.x) {
-      const float2 v = G[i];
-      A[i] = v;
-      const int r = (int)((sqrtf(8.f * (float)i + 1.f) - 1.f) * 0.5f);
-      const int rr = (r * (r + 1) / 2 > i) ? r - 1 : ((r + 1) * (r + 2) / 2 <= i ? r + 1 : r);
-      fro += (i - rr * (rr + 1) / 2 == rr ? 1.f : 2.f) * cabs2(v);
-    }
-    fro = block_sum(fro, misc->red);
-    // lambda_max <= ||G||_F: below lambda^2 every singular value is shrunk to zero.
-    const bool all_zero = !op.block_stat && op.mode != LLR_PROX_HARD_RANK && op.lambda > 0.f &&
-                          fro <= op.lambda * op.lambda * op.lambda * op.lambda;
-    if (!all_zero) hermitian_tridiag<NPMAX, true>(A, n, trd, misc->red);
-    if (op.block_stat) {
-      tridiag_setup<NPMAX>(trd, n, LLR_PROX_HARD_RANK, 1, 0.f, misc);
-      tridiag_eigenvalues<NPMAX>(trd, n, n - 1, 1, misc);
-      if (tid == 0) op.block_stat[blk] = trd->lam[0];
-      __syncthreads();
-      continue;
-    }
-    int ra = 0, nb = n;
-    if (!all_zero) {
-      tridiag_setup<NPMAX>(trd, n, op.mode, op.rank, op.lambda, misc);
-      ra = misc->ra;
-      nb = misc->n_below;
-    }
-    const bool identity = ra == n && op.mode == LLR_PROX_HARD_RANK;   // rank >= n
-    if (identity && !src.out) {
-      __syncthreads();
-      continue;
-    }
-    // row tables (only the apply needs them here)
-    for (int r = tid; r < m; r += blockDim.x) {
-      RowTab rt;
-      if (src.kind == 1) {
-        int ix, iy, iz;
-        block_row_coord(src, blk, sh, r, ix, iy, iz);
-        rt.off = (int)planar_index(src.g, ix, iy, iz, 0);
-        rt.cx = ix;
-        rt.cyz = iy | (iz << 16);
-        if (src.ph_uniform) rowph[r] = phase_at(src.ph, src.g, 0, ix, iy, iz);
-      } else {
-        rt.off = r;
-        rt.cx = 0;
-        rt.cyz = 0;
-      }
-      rt.pad = 0;
-      rows[r] = rt;
-    }
-    __syncthreads();
-    if (identity) {
-      copy_rows(src, base, rows, rowph, m, n, qstride);
-      __syncthreads();
-      continue;
-    }
-    if (ra == 0) {
-      if (!src.accumulate)
-        for (int idx = tid; idx < m * n; idx += blockDim.x) {
-          const int q = idx / m, r = idx - q * m;
-          store_elem(src, base, rows[r], rowph, r, q, qstride, make_float2(0.f, 0.f));
-        }
-      __syncthreads();
-      continue;
-    }
-    bool fallback = ra > kRaMax;
-    if (!fallback) {
-      tridiag_eigenvalues<NPMAX>(trd, n, nb, ra, misc);
-      tridiag_vectors<NPMAX>(trd, n, ra, misc, work);
-      fallback = misc->fail != 0;
-    }
-    if (fallback) {
-      if (tid == 0 && op.fb_list) {
-        const int pos = atomicAdd(op.fb_count, 1);
-        op.fb_list[pos] = (int)blk;
-      }
-      __syncthreads();
-      continue;
-    }
-    tridiag_backtransform<NPMAX, true>(A, trd, Va, n, ra);
-    if (tid < ra) {
-      float gv = 1.f;
-      if (op.mode != LLR_PROX_HARD_RANK) {
-        const float sv = sqrtf(fmaxf(trd->lam[tid], 0.f));
-        gv = (sv > op.lambda) ? (1.f - op.lambda / sv) : 0.f;
-      }
-      g[tid] = gv;
-    }
-    __syncthreads();
-    if (ra <= 4) apply_rows<4>(src, base, rows, rowph, m, n, qstride, Va, g, ra);
-    else if (ra <= 8) apply_rows<8>(src, base, rows, rowph, m, n, qstride, Va, g, ra);
-    else apply_rows<kRaMax>(src, base, rows, rowph, m, n, qstride, Va, g, ra);
-    __syncthreads();
-  }
-}
-
 // Soft-threshold apply with the refinement sweep: t_a = C v_a for the thread's (at most two)
 // rows, sigma_a^2 = ||C v_a||^2 / ||v_a||^2 summed over the block in FP64 (no Gram: the
 // conditioning is not squared), g_a = max(1 - lambda / sigma_a, 0), then C' = sum_a t_a g_a v_a^H.
 template <int RM>
 __device__ void apply_rows_refined(const BlockSource& s, long long base, const RowTab* rows, const float2* rowph,
                                    int m, int n, long long qstride, const float2* Va, float* g, int ra, float lam,
-                                   double* red) {
+                                   double* red, double* nucs, double* nuc_out) {
   constexpr int KB = 8;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
   float2 t[2][RM];
@@ -994,8 +859,14 @@ __device__ void apply_rows_refined(const BlockSource& s, long long base, const R
     }
     const double sig = vn > 0.0 ? sqrt(sum / vn) : 0.0;
     g[tid] = sig > (double)lam ? (float)(1.0 - (double)lam / sig) : 0.f;
+    nucs[tid] = sig > (double)lam ? sig - (double)lam : 0.0;
   }
   __syncthreads();
+  if (nuc_out && tid == 0) {   // the block's nuclear norm after the threshold, columns in order
+    double t = 0.0;
+    for (int a = 0; a < ra; ++a) t += nucs[a];
+    *nuc_out = t;
+  }
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
     const int r = tid + h * blockDim.x;
@@ -1019,7 +890,7 @@ __device__ void apply_rows_refined(const BlockSource& s, long long base, const R
 constexpr int kApplyThreads = 256;
 
 struct ApplyLayout {
-  size_t off_row, off_rowph, off_V, off_g, off_red, total;
+  size_t off_row, off_rowph, off_V, off_g, off_red, off_nuc, total;
 };
 
 inline ApplyLayout make_apply_layout(int m, int n) {
@@ -1030,6 +901,7 @@ inline ApplyLayout make_apply_layout(int m, int n) {
   L.off_V = off; off = align16(off + sizeof(float2) * (size_t)n * kFacCols);
   L.off_g = off; off = align16(off + sizeof(float) * kFacCols);
   L.off_red = off; off = align16(off + sizeof(double) * (kApplyThreads / 32) * kFacCols);
+  L.off_nuc = off; off = align16(off + sizeof(double) * kFacCols);
   L.total = off;
   return L;
 }
@@ -1042,6 +914,7 @@ __global__ void __launch_bounds__(kApplyThreads, 3) llr_apply_kernel(BlockSource
   float2* Va = reinterpret_cast<float2*>(smem + L.off_V);
   float* g = reinterpret_cast<float*>(smem + L.off_g);
   double* red = reinterpret_cast<double*>(smem + L.off_red);
+  double* nucs = reinterpret_cast<double*>(smem + L.off_nuc);
   const int m = op.m, n = op.n, tid = threadIdx.x;
   const long long qstride = src.kind == 1 ? src.g.V : (long long)m;
   // soft threshold: gains from ||C v||^2 (FP64 sum) when the block's rows fit two per thread
@@ -1079,6 +952,13 @@ __global__ void __launch_bounds__(kApplyThreads, 3) llr_apply_kernel(BlockSource
       if (tid < kFacCols) g[tid] = F[n * kFacCols + tid].x;
     }
     __syncthreads();
+    if (ra > 0 && !refine && op.blk_nuc && op.mode != LLR_PROX_HARD_RANK && tid == 0) {
+      // unrefined gains g = 1 - lambda / s: s - lambda = lambda g / (1 - g)
+      double t = 0.0;
+      for (int a = 0; a < ra; ++a)
+        if (g[a] > 0.f) t += (double)op.lambda * g[a] / (1.0 - (double)g[a]);
+      op.blk_nuc[blk] = t;
+    }
     if (ra == -2) {
       copy_rows(src, base, rows, rowph, m, n, qstride);
     } else if (ra == 0) {   // every singular value below the threshold: the block becomes zero
@@ -1087,9 +967,11 @@ __global__ void __launch_bounds__(kApplyThreads, 3) llr_apply_kernel(BlockSource
         for (int q = 0; q < n; ++q) rowp[(long long)q * qstride] = make_float2(0.f, 0.f);
       }
     } else if (refine) {
-      if (ra <= 2) apply_rows_refined<2>(src, base, rows, rowph, m, n, qstride, Va, g, ra, op.lambda, red);
-      else if (ra <= 4) apply_rows_refined<4>(src, base, rows, rowph, m, n, qstride, Va, g, ra, op.lambda, red);
-      else apply_rows_refined<kFacCols>(src, base, rows, rowph, m, n, qstride, Va, g, ra, op.lambda, red);
+      double* nuc = op.blk_nuc ? op.blk_nuc + blk : nullptr;
+      if (ra <= 2) apply_rows_refined<2>(src, base, rows, rowph, m, n, qstride, Va, g, ra, op.lambda, red, nucs, nuc);
+      else if (ra <= 4)
+        apply_rows_refined<4>(src, base, rows, rowph, m, n, qstride, Va, g, ra, op.lambda, red, nucs, nuc);
+      else apply_rows_refined<kFacCols>(src, base, rows, rowph, m, n, qstride, Va, g, ra, op.lambda, red, nucs, nuc);
     } else if (ra <= 2) {
       apply_rows<2, kFacCols>(src, base, rows, rowph, m, n, qstride, Va, g, ra);
     } else if (ra <= 4) {
@@ -1186,6 +1068,7 @@ __global__ void __launch_bounds__(kLlrThreads, 1) llr_prox_wide_kernel(BlockSour
       continue;
     }
     singular_map(A, lda, n, op.mode, op.rank, op.lambda, ev, g, act, misc);
+    if (op.blk_nuc && op.mode != LLR_PROX_HARD_RANK && tid == 0) op.blk_nuc[blk] = nuclear_from_eigs(ev, n, op.lambda);
     const int na = misc->n_active;
     const bool identity = na == n && op.mode == LLR_PROX_HARD_RANK;
     if (identity && !src.out) {
@@ -1273,23 +1156,8 @@ int launch_split_instance(const BlockSource& src, const ProxOp& op, cudaStream_t
     kern<<<(unsigned)grid, kLlrThreads, L.total, stream>>>(src, op, L);
     LLR_CUDA_TRY(cudaGetLastError());
   }
-  if (!op.block_stat && op.eig_solver == 0 && op.blk_ra) {   // warp eigen kernel + apply kernel
-    LLR_TRY(launch_llr_eig_warp(op, src.nblocks, stream));
-    return launch_apply(src, op, stream);
-  }
-  {
-    EigLayout L = make_eig_layout<NPMAX>(op.m);
-    auto kern = llr_eig_apply_kernel<NPMAX>;
-    LLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total));
-    LLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-    LLR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kEigThreads, L.total));
-    if (occ < 1) return set_error(LLR_ERR_UNSUPPORTED, "eigen kernel cannot be resident (smem %zu B)", L.total);
-    const long long grid = std::min<long long>(src.nblocks, (long long)nsm * occ);
-    note_launch();
-    kern<<<(unsigned)grid, kEigThreads, L.total, stream>>>(src, op, L);
-    LLR_CUDA_TRY(cudaGetLastError());
-  }
-  return LLR_OK;
+  LLR_TRY(launch_llr_eig_warp(op, src.nblocks, stream));
+  return launch_apply(src, op, stream);
 }
 
 }  // namespace
@@ -1324,7 +1192,10 @@ int launch_llr_prox(const BlockSource& src, const ProxOp& op, cudaStream_t strea
                                             "context or of an allocating entry point", op.n);
     return launch_prox_wide(src, op, stream);
   }
-  if (op.eig_solver == 1) return launch_llr_prox_jacobi(src, op, stream);
+  // the Jacobi kernel: every block when asked for, and the block statistics (largest Gram
+  // eigenvalue per block, sigma_max)
+  if (op.eig_solver == 1 || op.block_stat) return launch_llr_prox_jacobi(src, op, stream);
+  if (op.gram && !op.blk_ra) return set_error(LLR_ERR_INVALID, "split prox path needs the kept-count buffer");
   if (!op.block_stat && !op.fb_list)
     return set_error(LLR_ERR_INVALID, "tridiagonal prox needs a fallback block list");
   if (op.fb_count) LLR_CUDA_TRY(cudaMemsetAsync(op.fb_count, 0, sizeof(int), stream));

@@ -219,6 +219,23 @@ __global__ void __launch_bounds__(256) finalize_kernel(const double* partials, i
   }
 }
 
+// Objective of the iterate the prox just produced: 0.5 ||M A x - y||^2 (the residual the
+// finalize kernel stored for iteration k = *it - 1) plus lambda times the blocks' nuclear norms,
+// summed in FP64 in a fixed order.  blk_nuc null: the data term alone.
+__global__ void __launch_bounds__(256) objective_kernel(const double* blk_nuc, long long nb, double lam,
+                                                        const double* hist, double* obj, long long cap,
+                                                        const long long* it) {
+  __shared__ double sh[8];
+  double v = 0.0;
+  if (blk_nuc)
+    for (long long i = threadIdx.x; i < nb; i += 256) v += blk_nuc[i];
+  const double nuc = block_reduce_d<256>(v, sh);
+  if (threadIdx.x == 0) {
+    const long long k = *it - 1;
+    if (k >= 0 && k < cap) obj[k] = 0.5 * hist[k] + (blk_nuc ? lam * nuc : 0.0);
+  }
+}
+
 // sum |a - b|^2 and sum |b|^2 in FP64, one pair of partials per block
 __global__ void __launch_bounds__(256) diff_norm_kernel(const float2* __restrict__ a, const float2* __restrict__ b,
                                                         long long n, double* part_d, double* part_b) {
@@ -396,6 +413,14 @@ int launch_finalize(const double* partials, int np, double scale, double* hist, 
                     int advance, double* out, cudaStream_t s) {
   note_launch();
   finalize_kernel<<<1, 256, 0, s>>>(partials, np, scale, hist, cap, it, advance, out);
+  LLR_CUDA_TRY(cudaGetLastError());
+  return LLR_OK;
+}
+
+int launch_objective(const double* blk_nuc, long long nb, double lam, const double* hist, double* obj, long long cap,
+                     const long long* it, cudaStream_t s) {
+  note_launch();
+  objective_kernel<<<1, 256, 0, s>>>(blk_nuc, nb, lam, hist, obj, cap, it);
   LLR_CUDA_TRY(cudaGetLastError());
   return LLR_OK;
 }

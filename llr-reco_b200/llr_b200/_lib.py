@@ -113,6 +113,7 @@ SIGNATURES = {
     "llr_get_iteration": (C.c_int, [P, C.POINTER(I64)]),
     "llr_set_iteration": (C.c_int, [P, I64]),
     "llr_get_residual_history": (C.c_int, [P, PF64, I32]),
+    "llr_get_objective_history": (C.c_int, [P, PF64, I32]),
     "llr_measurement_stats": (C.c_int, [P, PF64, PF64]),
     "llr_sigma_max": (C.c_int, [P, PI32, PF64]),
     "llr_set_lambda": (C.c_int, [P, F32]),

@@ -252,6 +252,13 @@ class ReconContext:
         check(lib.llr_get_residual_history(self.h, h.ctypes.data_as(L.PF64), int(count)))
         return h
 
+    def objective_history(self, count: int) -> np.ndarray:
+        """0.5 ||M A x - y||^2 + lambda sum_b ||X_b||_* of the last ``count`` prox outputs (FP64;
+        NaN where the configuration defines no single objective)."""
+        h = np.empty(count, dtype=np.float64)
+        check(lib.llr_get_objective_history(self.h, h.ctypes.data_as(L.PF64), int(count)))
+        return h
+
     def measurement_stats(self) -> tuple[float, float]:
         e, u = C.c_double(), C.c_double()
         check(lib.llr_measurement_stats(self.h, C.byref(e), C.byref(u)))

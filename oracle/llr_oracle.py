@@ -712,6 +712,40 @@ def iterate(x: np.ndarray, y: np.ndarray, cfg: ReconConfig, it: int):
     return np.asfortranarray(xn), err
 
 
+def objective(z: np.ndarray, err: float, cfg: ReconConfig, shift) -> float:
+    """Objective of the prox output ``z`` of an iteration whose hard DC measured ``err`` =
+    ||M A z - y||^2: 0.5 err + lam sum_b ||Z_b||_* over the tiling at ``shift`` (soft threshold;
+    hard rank: 0.5 err).  Proximal gradient with step 1 (A unitary, lib.rs:262-341) minimises
+    this function; with a fixed tiling it decreases every iteration."""
+    if cfg.mode == "hard":
+        return 0.5 * err
+    nx, ny, nz, nq = z.shape
+    nb = int(np.prod(grid_dim((nx, ny, nz), cfg.block_size)))
+    if nb == 0:
+        return 0.5 * err
+    mats = lift_data_set(np.asfortranarray(z), cfg.block_size, shift, 0, nb)
+    return 0.5 * err + cfg.lam * float(block_singular_values(mats).sum())
+
+
+def recon_objective(y: np.ndarray, cfg: ReconConfig, n_iter: int, x0: Optional[np.ndarray] = None, it0: int = 0):
+    """``recon`` that also returns the objective of every iteration's prox output (plain soft or
+    hard LLR on one tiling: no wavelet, subspace or overlapping blocks)."""
+    assert cfg.wavelet_alpha <= 0 and cfg.subspace is None
+    assert cfg.block_stride is None or tuple(cfg.block_stride) == tuple(cfg.block_size)
+    x = zero_filled(y, cfg) if x0 is None else np.asfortranarray(x0.copy())
+    nx, ny, nz, nq = x.shape
+    hist, obj = [], []
+    for it in range(it0, it0 + n_iter):
+        shift = rand_shift(cfg.seed, it, cfg.max_rand_shift or (nx, ny, nz))
+        z = llr_prox(x, cfg, shift)
+        ksp, img = _corrections(cfg, nq)
+        k, err = hard_project(signal_model(z, ksp, img, FORWARD), y)
+        obj.append(objective(z, err, cfg, shift))
+        hist.append(err)
+        x = np.asfortranarray(signal_model(k, ksp, img, INVERSE))
+    return x, hist, obj
+
+
 def zero_filled(y: np.ndarray, cfg: ReconConfig) -> np.ndarray:
     """lib.rs:233-242: x0 = A^H y."""
     ksp, img = _corrections(cfg, y.shape[3])

@@ -59,7 +59,7 @@ def _cfg(**kw):
     (dict(nq=0), "nq"),
     (dict(max_rand_shift=(33, 1, 1)), "max_rand_shift"),
     (dict(subspace_rank=11), "subspace rank"),
-    (dict(eig_solver=3), "eig_solver"),
+    (dict(eig_solver=2), "eig_solver"),
     (dict(gram_mode=2), "gram_mode"),
     (dict(fft_mode=2), "fft_mode"),
 ])

@@ -80,7 +80,7 @@ def test_soft_threshold_hybrid_path(gpu):
     assert gh[-1] < gh[0]
 
 
-@pytest.mark.parametrize("eig_solver", [0, 1, 2])
+@pytest.mark.parametrize("eig_solver", [0, 1])
 def test_hard_rank_c1_like(gpu, eig_solver):
     """Config-1 shape class: 8^3 blocks, 17 volumes (Casorati 512 x 17), reduced volume."""
     d = dataset((32, 32, 32), 17, accel=4.0, centre=8)
@@ -88,7 +88,7 @@ def test_hard_rank_c1_like(gpu, eig_solver):
     check(gx, ox, gh, oh)
 
 
-@pytest.mark.parametrize("eig_solver,gram_mode", [(0, 0), (1, 0), (0, 1), (2, 0)])
+@pytest.mark.parametrize("eig_solver,gram_mode", [(0, 0), (1, 0), (0, 1)])
 def test_soft_c2_like(gpu, eig_solver, gram_mode):
     """Config-2 shape class: 6^3 blocks, 61 volumes (Casorati 216 x 61), reduced volume; both
     eigen-solvers (tridiagonal + bisection, Jacobi) and both Gram paths (3xTF32 tensor cores,
@@ -97,6 +97,63 @@ def test_soft_c2_like(gpu, eig_solver, gram_mode):
     gx, ox, gh, oh, _ = run_both(d.y, (6, 6, 6), L.LLR_PROX_SOFT_THRESH, 4, eig_solver=eig_solver,
                                  gram_mode=gram_mode)
     check(gx, ox, gh, oh)
+
+
+@pytest.mark.parametrize("nq,bs,max_shift,gram_mode", [(61, (6, 6, 6), None, 0), (17, (8, 8, 8), (1, 1, 1), 0),
+                                                       (9, (4, 4, 4), None, 1)])
+def test_objective_history_matches_oracle(gpu, nq, bs, max_shift, gram_mode):
+    """FP64 objective 0.5 ||M A x - y||^2 + lam sum_b ||X_b||_* of every iteration's prox output
+    against the oracle's (relative 2e-4, the complex-FP32 tolerance of the residual): random and
+    fixed partitions, both Gram paths (the nuclear norms come from the apply kernel's FP64
+    singular values and, for blocks the Jacobi kernel takes, its own)."""
+    d = dataset((24, 24, 16), nq, accel=4.0, centre=6)
+    ocfg = oracle_cfg(bs, "soft", seed=9, max_rand_shift=max_shift)
+    x0 = O.zero_filled(d.y.astype(np.complex128), ocfg)
+    ocfg.lam = 0.02 * O.sigma_max(x0, bs)
+    p = ReconParams(vol_size=(24, 24, 16), nq=nq, block_size=bs, prox_mode=L.LLR_PROX_SOFT_THRESH, lam=ocfg.lam,
+                    seed=9, max_rand_shift=max_shift, gram_mode=gram_mode)
+    with ReconContext(p) as ctx:
+        ctx.upload_kspace(d.y)
+        ctx.init_zero_filled()
+        hist = ctx.iterate(4)
+        obj = ctx.objective_history(4)
+    _, oh, oo = O.recon_objective(d.y.astype(np.complex128), ocfg, 4, x0=x0)
+    np.testing.assert_allclose(hist, oh, rtol=2e-4)
+    np.testing.assert_allclose(obj, oo, rtol=2e-4)
+
+
+def test_objective_monotone_with_fixed_partition(gpu):
+    """With the tiling fixed the objective never rises (proximal gradient, step 1, unitary A):
+    60 iterations on the GPU, each step checked, allowing an FP32-level relative 1e-6 wobble;
+    the hard-rank objective is half the residual; a wavelet run has none (NaN)."""
+    d = dataset((24, 24, 16), 17, accel=4.0, centre=6)
+    ocfg = oracle_cfg((6, 6, 4), "soft", seed=4, max_rand_shift=(1, 1, 1))
+    lam = 0.02 * O.sigma_max(O.zero_filled(d.y.astype(np.complex128), ocfg), (6, 6, 4))
+    p = ReconParams(vol_size=(24, 24, 16), nq=17, block_size=(6, 6, 4), prox_mode=L.LLR_PROX_SOFT_THRESH, lam=lam,
+                    seed=4, max_rand_shift=(1, 1, 1))
+    with ReconContext(p) as ctx:
+        ctx.upload_kspace(d.y)
+        ctx.init_zero_filled()
+        ctx.iterate(60)
+        obj = ctx.objective_history(60)
+    assert np.all(np.isfinite(obj))
+    assert np.all(obj[1:] <= obj[:-1] * (1 + 1e-6)), np.diff(obj).max()
+    assert obj[-1] < 0.99 * obj[0]
+    ph = ReconParams(vol_size=(24, 24, 16), nq=17, block_size=(6, 6, 4), prox_mode=L.LLR_PROX_HARD_RANK, rank=2,
+                     seed=4)
+    with ReconContext(ph) as ctx:
+        ctx.upload_kspace(d.y)
+        ctx.init_zero_filled()
+        h = ctx.iterate(3)
+        np.testing.assert_array_equal(ctx.objective_history(3), 0.5 * np.asarray(h))
+    pw = ReconParams(vol_size=(24, 24, 16), nq=17, block_size=(6, 6, 4), prox_mode=L.LLR_PROX_SOFT_THRESH, lam=lam,
+                     seed=4)
+    pw.wavelet_alpha, pw.wavelet_moments, pw.wavelet_levels = 0.005, 2, 1
+    with ReconContext(pw) as ctx:
+        ctx.upload_kspace(d.y)
+        ctx.init_zero_filled()
+        ctx.iterate(2)
+        assert np.all(np.isnan(ctx.objective_history(2)))
 
 
 @pytest.mark.parametrize("vol,fft_mode", [((16, 24, 12), 0), ((16, 24, 12), 1), ((6, 48, 32), 0)])
