@@ -15,6 +15,7 @@ single converged image to measure against.
 from __future__ import annotations
 
 import ctypes as C
+import json
 from dataclasses import dataclass, field
 from typing import Optional, Sequence
 
@@ -81,6 +82,14 @@ def reference(proto: Protocol, y: np.ndarray, n_iter: int, snapshot: bool = Fals
         if snapshot:
             return x_zf, ctx.download_image(), lam, energy, ctx.snapshot()
         return x_zf, ctx.download_image(), lam, energy
+
+
+def start_state(proto: Protocol, y: np.ndarray):
+    """Zero-filled image, lambda = lam_rel * sigma_max of it and the measured k-space energy."""
+    with ReconContext(proto.params()) as ctx:
+        ctx.upload_kspace(y)
+        ctx.init_zero_filled()
+        return ctx.download_image(), proto.lam_rel * ctx.sigma_max((0, 0, 0)), ctx.measurement_stats()[0]
 
 
 def calibration_kspace(proto: Protocol, y: np.ndarray) -> np.ndarray:
@@ -228,6 +237,137 @@ def time_to_targets(proto: Protocol, y: np.ndarray, lam: float, x_start: np.ndar
     return res, curve
 
 
+def _synth_kspace(args):
+    """Worker of the synthesis pool: the measured k-space of one subject (host only)."""
+    vol, shells, accel, seed, centre, protocol_seed = args
+    return make_dataset(vol, shells, accel, seed, centre=centre, protocol_seed=protocol_seed).y
+
+
+def subject_stream(proto: Protocol, seeds: Sequence[int], workers: int):
+    """Yields (seed, y) in order; the phantoms are synthesised on ``workers`` host processes
+    (started with spawn, so they hold no CUDA state) while the caller uses the GPU."""
+    args = [(tuple(proto.vol), proto.shells, proto.accel, int(s), proto.centre, proto.protocol_seed) for s in seeds]
+    if workers <= 1:
+        for a in args:
+            yield a[3], _synth_kspace(a)
+        return
+    import multiprocessing as mp
+    with mp.get_context("spawn").Pool(workers) as pool:
+        for a, y in zip(args, pool.imap(_synth_kspace, args, chunksize=1)):
+            yield a[3], y
+
+
+def objective_run(proto: Protocol, y: np.ndarray, lam: float, x_start: Optional[np.ndarray], n_iter: int,
+                  gram_mode: Optional[int] = None):
+    """n_iter fixed-partition iterations from x_start (None: the zero-filled image); returns the
+    objective of every iteration (FP64, ReconContext.objective_history) and the device ms."""
+    p = proto.params(lam)
+    if gram_mode is not None:
+        p.gram_mode = gram_mode
+    with ReconContext(p) as ctx:
+        ctx.upload_kspace(y)
+        if x_start is None:
+            ctx.init_zero_filled()
+        else:
+            ctx.upload_image(x_start)
+        ctx.iteration = 0
+        ms = ctx.iterate_timed(n_iter)
+        obj = ctx.objective_history(n_iter)
+    return obj, ms
+
+
+def iterations_to(obj: np.ndarray, f_star: float, tol: float) -> Optional[int]:
+    """First iteration count k with F_k <= F* + tol |F*| (None: never within the run)."""
+    hit = np.flatnonzero(obj <= f_star + tol * abs(f_star))
+    return int(hit[0]) + 1 if hit.size else None
+
+
+def protocol_eval(net: Cnn, proto: Protocol, codec: SubspaceCodec, seeds: Sequence[int], n_conv: int, tol: float,
+                  workers: int, log=print) -> dict:
+    """The learned start judged on held-out subjects: for each, the plain FP32 method (FMA Gram)
+    and the mixed-precision method (3xTF32 tensor-core Gram) from the zero-filled image, and the
+    mixed method from the network's image, each run n_conv fixed-partition iterations; F* is the
+    lowest objective any of the three reached; reported are the iterations and device seconds
+    until F_k <= F* + tol |F*| (the network's time included in the learned run)."""
+    per = []
+    for seed, y in subject_stream(proto, seeds, workers):
+        x_zf, lam, energy = start_state(proto, y)
+        x0, net_ms = warm_start_image(net, codec, x_zf, energy, y)
+        runs = {"plain_fp32": objective_run(proto, y, lam, None, n_conv, gram_mode=1),
+                "plain_mixed": objective_run(proto, y, lam, None, n_conv, gram_mode=0),
+                "learned_mixed": objective_run(proto, y, lam, x0, n_conv, gram_mode=0)}
+        f_star = min(float(np.nanmin(o)) for o, _ in runs.values())
+        rec = {"seed": int(seed), "f_star": f_star, "network_ms": round(net_ms, 3),
+               "tail_change": float(abs(runs["plain_mixed"][0][-101] - runs["plain_mixed"][0][-1]) / abs(f_star))}
+        for name, (o, ms) in runs.items():
+            k = iterations_to(o, f_star, tol)
+            t_it = ms / n_conv
+            extra = net_ms if name == "learned_mixed" else 0.0
+            rec[name] = {"iterations": k, "ms_per_iteration": round(t_it, 4),
+                         "seconds": None if k is None else round(1e-3 * (k * t_it + extra), 5),
+                         "start_gap": float((o[0] - f_star) / abs(f_star))}
+        log(json.dumps(rec))
+        per.append(rec)
+
+    def stat(key, field):
+        v = [r[key][field] for r in per if r[key][field] is not None]
+        return {"median": float(np.median(v)), "mean": float(np.mean(v)), "n": len(v)} if v else None
+
+    summary = {k: {"iterations": stat(k, "iterations"), "seconds": stat(k, "seconds")}
+               for k in ("plain_fp32", "plain_mixed", "learned_mixed")}
+    ratios = [r["plain_fp32"]["seconds"] / r["learned_mixed"]["seconds"] for r in per
+              if r["plain_fp32"]["seconds"] and r["learned_mixed"]["seconds"]]
+    it_ratio = [r["plain_mixed"]["iterations"] / r["learned_mixed"]["iterations"] for r in per
+                if r["plain_mixed"]["iterations"] and r["learned_mixed"]["iterations"]]
+    summary["speedup_learned_mixed_vs_plain_fp32"] = {"median": float(np.median(ratios)),
+                                                      "min": float(np.min(ratios)), "max": float(np.max(ratios))} \
+        if ratios else None
+    summary["iteration_ratio_zero_filled_vs_learned"] = {"median": float(np.median(it_ratio)),
+                                                         "min": float(np.min(it_ratio)),
+                                                         "max": float(np.max(it_ratio))} if it_ratio else None
+    summary["learned_fewer_iterations"] = sum(
+        1 for r in per if r["plain_mixed"]["iterations"] and r["learned_mixed"]["iterations"]
+        and r["learned_mixed"]["iterations"] < r["plain_mixed"]["iterations"])
+    return {"subjects": per, "summary": summary}
+
+
+def run_protocol(a) -> dict:
+    """Training on ``a.train`` seeded phantoms reconstructed by the plain method (``a.n_ref``
+    fixed-partition iterations), then the held-out evaluation (protocol_eval)."""
+    import time
+    proto = Protocol(vol=tuple(a.vol), centre=a.centre)
+    codec = SubspaceCodec(proto)
+    t0 = time.time()
+    pairs = []
+    for seed, y in subject_stream(proto, range(a.train_seed0, a.train_seed0 + a.train), a.workers):
+        x_zf, x_ref, _, energy = reference(proto, y, a.n_ref)
+        sc = channel_scale(proto, energy)
+        ph = calibration_image(proto, y)
+        pairs.append((codec.channels(x_zf, sc, ph), codec.channels(x_ref, sc, ph)))
+        if ph is not None:
+            ph.close()
+    t1 = time.time()
+    net = Cnn(seed=a.seed)
+    losses = train(net, pairs, a.epochs, a.lr)
+    t2 = time.time()
+    for xin, tgt in pairs:
+        xin.close()
+        tgt.close()
+    ev = protocol_eval(net, proto, codec, range(a.test_seed0, a.test_seed0 + a.test), a.n_conv, a.tol, a.workers)
+    t3 = time.time()
+    info = dict(vol=list(proto.vol), shells=proto.shells, accel=proto.accel, block=list(proto.block),
+                centre=proto.centre, train_subjects=a.train, n_ref=a.n_ref, epochs=a.epochs, lr=a.lr, seed=a.seed,
+                test_subjects=a.test, n_conv=a.n_conv, tol=a.tol, loss_first=losses[0], loss_last=losses[-1],
+                pairs_s=round(t1 - t0, 1), train_s=round(t2 - t1, 1), eval_s=round(t3 - t2, 1))
+    if a.weights:
+        import os
+        os.makedirs(os.path.dirname(os.path.abspath(a.weights)), exist_ok=True)
+        np.savez(a.weights, channels=np.asarray(net.channels, dtype=np.int32), params=net.params,
+                 info=np.asarray(json.dumps(info)))
+    net.close()
+    return {"protocol": info, **ev}
+
+
 def default_weights_path() -> str:
     import os
     return os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "warm_start_net.npz")
@@ -240,7 +380,7 @@ def main(argv=None) -> None:
     import json
     import time
     ap = argparse.ArgumentParser(description=main.__doc__)
-    ap.add_argument("cmd", choices=["train"])
+    ap.add_argument("cmd", choices=["train", "protocol"])
     ap.add_argument("--out", default=default_weights_path())
     ap.add_argument("--vol", type=int, nargs=3, default=[96, 96, 48])
     ap.add_argument("--centre", type=int, default=8)
@@ -249,7 +389,28 @@ def main(argv=None) -> None:
     ap.add_argument("--epochs", type=int, default=40)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=5)
+    # protocol: train on --train subjects (--n-ref plain iterations each), judge on --test held-out
+    ap.add_argument("--train", type=int, default=200)
+    ap.add_argument("--test", type=int, default=20)
+    ap.add_argument("--train-seed0", type=int, default=10000)
+    ap.add_argument("--test-seed0", type=int, default=20000)
+    ap.add_argument("--n-conv", type=int, default=1000)
+    ap.add_argument("--tol", type=float, default=1e-4)
+    ap.add_argument("--workers", type=int, default=0, help="synthesis processes (0: host cores - 1, at most 32)")
+    ap.add_argument("--weights", default=None, help="protocol: where to write the trained parameters")
+    ap.add_argument("--report", default=None, help="protocol: JSON report path")
     a = ap.parse_args(argv)
+    if a.cmd == "protocol":
+        import os
+        if a.workers <= 0:
+            a.workers = max(1, min(32, len(os.sched_getaffinity(0)) - 1))
+        rep = run_protocol(a)
+        txt = json.dumps(rep, indent=1)
+        if a.report:
+            with open(a.report, "w") as f:
+                f.write(txt)
+        print(json.dumps({"protocol": rep["protocol"], "summary": rep["summary"]}))
+        return
     proto = Protocol(vol=tuple(a.vol), centre=a.centre)
     codec = SubspaceCodec(proto)
     t0 = time.time()
