@@ -245,16 +245,24 @@ def _synth_kspace(args):
 
 def subject_stream(proto: Protocol, seeds: Sequence[int], workers: int):
     """Yields (seed, y) in order; the phantoms are synthesised on ``workers`` host processes
-    (started with spawn, so they hold no CUDA state) while the caller uses the GPU."""
+    (started with spawn, so they hold no CUDA state) while the caller uses the GPU.  At most
+    ``workers`` finished or running subjects are outstanding, which bounds host memory."""
     args = [(tuple(proto.vol), proto.shells, proto.accel, int(s), proto.centre, proto.protocol_seed) for s in seeds]
     if workers <= 1:
         for a in args:
             yield a[3], _synth_kspace(a)
         return
+    import collections
     import multiprocessing as mp
     with mp.get_context("spawn").Pool(workers) as pool:
-        for a, y in zip(args, pool.imap(_synth_kspace, args, chunksize=1)):
-            yield a[3], y
+        pending = collections.deque()
+        nxt = 0
+        while nxt < len(args) or pending:
+            while nxt < len(args) and len(pending) < workers:
+                pending.append((args[nxt][3], pool.apply_async(_synth_kspace, (args[nxt],))))
+                nxt += 1
+            seed, res = pending.popleft()
+            yield seed, res.get()
 
 
 def objective_run(proto: Protocol, y: np.ndarray, lam: float, x_start: Optional[np.ndarray], n_iter: int,
@@ -396,14 +404,14 @@ def main(argv=None) -> None:
     ap.add_argument("--test-seed0", type=int, default=20000)
     ap.add_argument("--n-conv", type=int, default=1000)
     ap.add_argument("--tol", type=float, default=1e-4)
-    ap.add_argument("--workers", type=int, default=0, help="synthesis processes (0: host cores - 1, at most 32)")
+    ap.add_argument("--workers", type=int, default=0, help="synthesis processes (0: half the host cores, at most 8)")
     ap.add_argument("--weights", default=None, help="protocol: where to write the trained parameters")
     ap.add_argument("--report", default=None, help="protocol: JSON report path")
     a = ap.parse_args(argv)
     if a.cmd == "protocol":
         import os
         if a.workers <= 0:
-            a.workers = max(1, min(32, len(os.sched_getaffinity(0)) - 1))
+            a.workers = max(1, min(8, len(os.sched_getaffinity(0)) // 2))
         rep = run_protocol(a)
         txt = json.dumps(rep, indent=1)
         if a.report:
