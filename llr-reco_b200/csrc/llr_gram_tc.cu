@@ -133,6 +133,11 @@ __global__ void __launch_bounds__(kTcThreads, 3) llr_gram_tc_kernel(BlockSource 
   // one chunk: wait for its operand buffer, convert `pre` into it, refill `pre` two chunks
   // ahead, hand the buffer to the tensor core
   int gpar = 0;
+  // operand offsets of this thread's elements: row q = warp + kTcWarps t (and n + q), column
+  // lane; adding 8 to a row leaves its swizzle phase and moves it one 1 KB atom on, so
+  // op_offset(q + 8 t, lane) = op_offset(q, lane) + 1024 t
+  static_assert(kTcWarps == 8, "the 1 KB step per t assumes rows 8 apart");
+  const int oq0 = op_offset(warp, lane), oi0 = op_offset(n + warp, lane);
   auto step = [&](float2 (&pre)[kQT], long long blk, int j, int c) -> bool {
     const int b = gpar;
     if (used[b]) {  // the MMAs that read this buffer two chunks ago must be done
@@ -160,7 +165,7 @@ __global__ void __launch_bounds__(kTcThreads, 3) llr_gram_tc_kernel(BlockSource 
         x = cscale(cmul_bc(x, p), src.load_scale);
       }
       const uint32_t a = tf32_rna(x.x), bb = tf32_rna(x.y);
-      const int oq = op_offset(q, lane), oi = op_offset(n + q, lane);
+      const int oq = oq0 + 1024 * t, oi = oi0 + 1024 * t;
       *reinterpret_cast<uint32_t*>(hi + oq) = a;
       *reinterpret_cast<uint32_t*>(hi + oi) = bb;
       *reinterpret_cast<uint32_t*>(lo + oq) = __float_as_uint(x.x - __uint_as_float(a));
