@@ -404,6 +404,42 @@ def test_near_threshold_gains_refined(gpu):
         assert err < 1e-4 * lam, (b, err, s[:4])
 
 
+def test_near_threshold_vector_error_bounded(gpu):
+    """The refinement sweep fixes gains, not vectors: the eigenvectors still come from the FP32-level
+    Gram, whose eigenvalues carry an absolute error ~ eps sigma_1^2.  Bound what that leaves, on the
+    construction above (sigma_1 = 40 lambda beside singular values within 0.2 % of lambda):
+    * the whole output, not only its projection on the near-threshold vectors: ||C' - C'_64||_F
+      <= 2e-4 lambda per block;
+    * the dominant right singular vector (gap sigma_1^2 - 1 ~ 1600 lambda^2, so its perturbation is
+      ~ eps): sin of its angle to the FP64 one <= 1e-5;
+    * the near-threshold vectors may turn inside their cluster by ~ eps sigma_1^2 / gap (gap ~ 3e-3
+      lambda^2 here, a few per cent), but not out of it: the output's component outside the span of
+      the FP64 kept vectors (sigma > lambda) is <= 2e-4 lambda."""
+    rng = np.random.default_rng(37)
+    m, n, lam = 216, 61, 1.0
+    sig = [[40.0, 1.0 + 2e-3, 1.0 - 2e-3, 1.0 + 5e-4] + list(rng.uniform(0.05, 0.6, n - 4)) for _ in range(12)]
+    A = _spectrum_blocks(rng, m, n, sig).astype(np.complex64)
+    d = DeviceBuffer.from_array(A)
+    L.check(L.lib.llr_soft_threshold_batch_dev(m, n, lam, A.shape[2], d.ptr, None))
+    got = d.download(np.empty_like(A, order="F")).astype(np.complex128)
+    A64 = A.astype(np.complex128)
+    exp = O.low_rank_soft(A64, lam)
+    worst = [0.0, 0.0, 0.0]
+    for b in range(A.shape[2]):
+        _, s, Vh = np.linalg.svd(A64[:, :, b], full_matrices=False)
+        full = np.linalg.norm(got[:, :, b] - exp[:, :, b])
+        _, _, Vg = np.linalg.svd(got[:, :, b], full_matrices=False)
+        sin1 = np.sqrt(max(0.0, 1.0 - abs(np.vdot(Vh[0], Vg[0])) ** 2))
+        kept = Vh[s > lam].conj().T                  # FP64 kept right singular vectors
+        outside = np.linalg.norm(got[:, :, b] - got[:, :, b] @ kept @ kept.conj().T)
+        worst = [max(worst[0], full), max(worst[1], sin1), max(worst[2], outside)]
+    print(f"near-threshold blocks: max ||C' - C'_64||_F {worst[0]:.2e} lambda, max sin(v1) {worst[1]:.2e}, "
+          f"max component outside the kept span {worst[2]:.2e} lambda")
+    assert worst[0] <= 2e-4 * lam, worst
+    assert worst[1] <= 1e-5, worst
+    assert worst[2] <= 2e-4 * lam, worst
+
+
 def test_subspace_construction_matches_oracle(gpu):
     """GPU temporal subspace (simulated signals, FP64 Gram, FP64 Jacobi) against the oracle's
     restatement with the same counter-based draws: the same subspace and singular values."""
