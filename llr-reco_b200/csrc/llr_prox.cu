@@ -206,7 +206,8 @@ __global__ void __launch_bounds__(kLlrThreads) llr_subspace_kernel(BlockSource s
     }
     __syncthreads();
     gram<NPMAX, 2>(Z, L.ldc, m, sr, A, scr, L.ksplit);
-    jacobi<NPMAX>(A, V, sr, rot, pairs, misc, 16);
+    if (threadIdx.x < 32) jacobi_warp<NPMAX>(A, V, sr, rot, pairs, misc, 16);
+    __syncthreads();
     singular_map(A, lda, sr, op.mode, op.rank, op.lambda, ev, g, act, misc);
     form_W(A, V, lda, sr, g, act, misc->n_active);
     apply_W<NPMAX, 2>(Z, L.ldc, m, sr, A);
@@ -283,7 +284,8 @@ __global__ void __launch_bounds__(kLlrThreads) llr_subspace_coef_kernel(BlockSou
     }
     __syncthreads();
     gram<NPMAX, 2>(Z, L.ldc, m, sr, A, scr, L.ksplit);
-    jacobi<NPMAX>(A, V, sr, rot, pairs, misc, 16);
+    if (threadIdx.x < 32) jacobi_warp<NPMAX>(A, V, sr, rot, pairs, misc, 16);
+    __syncthreads();
     singular_map(A, NPMAX + 1, sr, op.mode, op.rank, op.lambda, ev, g, act, misc);
     form_W(A, V, NPMAX + 1, sr, g, act, misc->n_active);
     apply_W<NPMAX, 2>(Z, L.ldc, m, sr, A);

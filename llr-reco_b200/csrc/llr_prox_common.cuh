@@ -287,6 +287,108 @@ __device__ void jacobi(float2* A, float2* V, int n, float4* rot, int2* pairs, Mi
   }
 }
 
+// The same cyclic Jacobi run by one warp (the calling warp's lanes; warp barriers only), for the
+// small matrices of the subspace prox (n <= 16): the rotations of a step are a handful, and the
+// CTA-wide version spent most of its time in block barriers.  Call it from one whole warp with
+// the CTA synchronised before and after.
+template <int NPMAX>
+__device__ void jacobi_warp(float2* A, float2* V, int n, float4* rot, int2* pairs, Misc* misc, int max_sweeps,
+                       int lda = NPMAX + 1) {
+  const int tid = threadIdx.x & 31;
+  const int n2 = (n + 1) & ~1;
+  const int half = n2 >> 1;
+  const int M = n2 - 1;
+  for (int idx = tid; idx < n2 * n2; idx += 32) {
+    int i = idx / n2, j = idx - i * n2;
+    V[i * lda + j] = make_float2(i == j ? 1.f : 0.f, 0.f);
+  }
+  float loc = 0.f;
+  for (int idx = tid; idx < n * n; idx += 32) {
+    int i = idx / n, j = idx - i * n;
+    loc += cabs2(A[i * lda + j]);
+  }
+  for (int o = 16; o > 0; o >>= 1) loc += __shfl_xor_sync(0xffffffffu, loc, o);
+  const float fro2 = loc;
+  if (tid == 0) { misc->normF = sqrtf(fro2); misc->flag[0] = 0; misc->flag[1] = 0; }
+  __syncwarp();
+  const float thr = 2.4e-7f * misc->normF;
+  if (n2 < 2 || !(misc->normF > 0.f)) return;
+
+  for (int sweep = 0; sweep < max_sweeps; ++sweep) {
+    const int fs = sweep & 1;
+    for (int step = 0; step < M; ++step) {
+      if (tid < half) {
+        const int k = tid;
+        int p, q;
+        if (k == 0) { p = step; q = M; }
+        else { p = (step + k) % M; q = (step - k + M) % M; }
+        if (p > q) { int t = p; p = q; q = t; }
+        float c = 1.f, s = 0.f, ex = 1.f, ey = 0.f;
+        if (q < n) {
+          const float app = A[p * lda + p].x, aqq = A[q * lda + q].x;
+          const float2 apq = A[p * lda + q];
+          const float r = hypotf(apq.x, apq.y);
+          if (r > thr) {
+            const float tau = (aqq - app) / (2.f * r);
+            float t;
+            if (fabsf(tau) > 1e15f) t = 0.5f / tau;
+            else t = copysignf(1.f, tau) / (fabsf(tau) + sqrtf(1.f + tau * tau));
+            c = rsqrtf(1.f + t * t);
+            s = t * c;
+            ex = apq.x / r; ey = apq.y / r;
+            misc->flag[fs] = 1;
+          }
+        }
+        rot[k] = make_float4(c, s, ex, ey);
+        pairs[k] = make_int2(p, q);
+      }
+      __syncwarp();
+      if (step == 0 && tid == 0) misc->flag[fs ^ 1] = 0;
+      for (int b = tid; b < half * half; b += 32) {
+        const int k1 = b / half, k2 = b - k1 * half;
+        const int2 P1 = pairs[k1], P2 = pairs[k2];
+        const float4 R1 = rot[k1], R2 = rot[k2];
+        const bool id1 = (R1.y == 0.f), id2 = (R2.y == 0.f);
+        if (id1 && id2) continue;
+        const float2 e1 = make_float2(R1.z, R1.w);
+        const float2 e2c = make_float2(R2.z, -R2.w);
+        float2 a11 = A[P1.x * lda + P2.x], a12 = A[P1.x * lda + P2.y];
+        float2 a21 = A[P1.y * lda + P2.x], a22 = A[P1.y * lda + P2.y];
+        if (!id2) {  // columns: [x_p, x_q] J2,  J2 = [[c, s], [-s e2*, c e2*]]
+          float2 t12 = cmul(a12, e2c), t22 = cmul(a22, e2c);
+          float2 b11 = make_float2(R2.x * a11.x - R2.y * t12.x, R2.x * a11.y - R2.y * t12.y);
+          float2 b12 = make_float2(R2.y * a11.x + R2.x * t12.x, R2.y * a11.y + R2.x * t12.y);
+          float2 b21 = make_float2(R2.x * a21.x - R2.y * t22.x, R2.x * a21.y - R2.y * t22.y);
+          float2 b22 = make_float2(R2.y * a21.x + R2.x * t22.x, R2.y * a21.y + R2.x * t22.y);
+          a11 = b11; a12 = b12; a21 = b21; a22 = b22;
+        }
+        if (!id1) {  // rows: J1^H [row_p; row_q],  J1^H = [[c, -s e1], [s, c e1]]
+          float2 t21 = cmul(e1, a21), t22 = cmul(e1, a22);
+          float2 n11 = make_float2(R1.x * a11.x - R1.y * t21.x, R1.x * a11.y - R1.y * t21.y);
+          float2 n12 = make_float2(R1.x * a12.x - R1.y * t22.x, R1.x * a12.y - R1.y * t22.y);
+          float2 n21 = make_float2(R1.y * a11.x + R1.x * t21.x, R1.y * a11.y + R1.x * t21.y);
+          float2 n22 = make_float2(R1.y * a12.x + R1.x * t22.x, R1.y * a12.y + R1.x * t22.y);
+          a11 = n11; a12 = n12; a21 = n21; a22 = n22;
+        }
+        if (k1 == k2) { a12 = make_float2(0.f, 0.f); a21 = a12; a11.y = 0.f; a22.y = 0.f; }
+        A[P1.x * lda + P2.x] = a11; A[P1.x * lda + P2.y] = a12;
+        A[P1.y * lda + P2.x] = a21; A[P1.y * lda + P2.y] = a22;
+        if (!id2) {  // V <- V J2 on rows P1 x columns P2
+          float2 v11 = V[P1.x * lda + P2.x], v12 = V[P1.x * lda + P2.y];
+          float2 v21 = V[P1.y * lda + P2.x], v22 = V[P1.y * lda + P2.y];
+          float2 t12 = cmul(v12, e2c), t22 = cmul(v22, e2c);
+          V[P1.x * lda + P2.x] = make_float2(R2.x * v11.x - R2.y * t12.x, R2.x * v11.y - R2.y * t12.y);
+          V[P1.x * lda + P2.y] = make_float2(R2.y * v11.x + R2.x * t12.x, R2.y * v11.y + R2.x * t12.y);
+          V[P1.y * lda + P2.x] = make_float2(R2.x * v21.x - R2.y * t22.x, R2.x * v21.y - R2.y * t22.y);
+          V[P1.y * lda + P2.y] = make_float2(R2.y * v21.x + R2.x * t22.x, R2.y * v21.y + R2.x * t22.y);
+        }
+      }
+      __syncwarp();
+    }
+    if (misc->flag[fs] == 0) break;
+  }
+}
+
 // g(lambda) for every eigenvalue and the compacted list of active eigenvectors.
 __device__ void singular_map(const float2* A, int lda, int n, int mode, int rank, float lam, float* ev, float* g,
                              int* act, Misc* misc) {

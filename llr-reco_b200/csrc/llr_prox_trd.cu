@@ -1192,9 +1192,12 @@ int launch_llr_prox(const BlockSource& src, const ProxOp& op, cudaStream_t strea
                                             "context or of an allocating entry point", op.n);
     return launch_prox_wide(src, op, stream);
   }
-  // the Jacobi kernel: every block when asked for, and the block statistics (largest Gram
-  // eigenvalue per block, sigma_max)
-  if (op.eig_solver == 1 || op.block_stat) return launch_llr_prox_jacobi(src, op, stream);
+  if (op.eig_solver == 1) return launch_llr_prox_jacobi(src, op, stream);   // every block by Jacobi
+  if (op.block_stat) {   // largest Gram eigenvalue per block (sigma_max): fused kernel, chunked Gram, any m
+    if (op.n <= 16) return launch_trd_instance<16, 2>(src, op, stream);
+    if (op.n <= 32) return launch_trd_instance<32, 2>(src, op, stream);
+    return launch_trd_instance<64, 4>(src, op, stream);
+  }
   if (op.gram && !op.blk_ra) return set_error(LLR_ERR_INVALID, "split prox path needs the kept-count buffer");
   if (!op.block_stat && !op.fb_list)
     return set_error(LLR_ERR_INVALID, "tridiagonal prox needs a fallback block list");

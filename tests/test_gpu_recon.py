@@ -122,6 +122,27 @@ def test_objective_history_matches_oracle(gpu, nq, bs, max_shift, gram_mode):
     np.testing.assert_allclose(obj, oo, rtol=2e-4)
 
 
+@pytest.mark.parametrize("bs,srank", [((6, 6, 6), 0), ((8, 8, 8), 7)])
+def test_sigma_max_large_blocks(gpu, bs, srank):
+    """sigma_max (the lambda scale) of 61-volume blocks, 216 x 61 without a subspace and 512 x 61 with
+    one (the config-3 block, too large to stage whole in shared memory), against the oracle's FP64
+    SVD of every block."""
+    from llr_b200.phantom import dti_subspace
+    d = dataset((24, 24, 24), 61, accel=4.0, centre=6)
+    x0 = O.zero_filled(d.y.astype(np.complex128), oracle_cfg(bs, "soft"))
+    p = ReconParams(vol_size=(24, 24, 24), nq=61, block_size=bs, prox_mode=L.LLR_PROX_SOFT_THRESH, lam=1.0,
+                    subspace_rank=srank)
+    with ReconContext(p) as ctx:
+        ctx.upload_kspace(d.y)
+        if srank:
+            ctx.upload_subspace(dti_subspace(d.b, d.g, srank, 5000, 1))
+        ctx.init_zero_filled()
+        for sh in ((0, 0, 0), (3, 5, 1)):
+            s = ctx.sigma_max(sh)
+            e = O.sigma_max(x0, bs, sh)
+            assert abs(s - e) <= 1e-5 * e, (sh, s, e)
+
+
 def test_objective_monotone_with_fixed_partition(gpu):
     """With the tiling fixed the objective never rises (proximal gradient, step 1, unitary A):
     60 iterations on the GPU, each step checked, allowing an FP32-level relative 1e-6 wobble;
