@@ -381,7 +381,7 @@ int llr_ctx_create(const llr_config* cfg, llr_ctx** out) {
   if ((st = dalloc(&c->d_block_stat, (size_t)std::max<long long>(1, c->nblocks)))) return fail(st);
   if ((st = dalloc(&c->d_fb, (size_t)std::max<long long>(1, c->nblocks) + 1))) return fail(st);
   if ((st = dalloc(&c->d_err, 1))) return fail(st);
-  if (cfg->subspace_rank == 0 && c->g.nq > 64) {
+  if (cfg->subspace_rank == 0 && (c->g.nq > 64 || prox_needs_wide_fallback(c->m, c->g.nq))) {
     c->vwide_ctas = wide_jacobi_ctas();
     if ((st = dalloc(&c->d_vwide, (size_t)c->vwide_ctas * (size_t)wide_v_stride()))) return fail(st);
   }

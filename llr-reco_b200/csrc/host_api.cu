@@ -391,7 +391,7 @@ static int batch_prox(int m, int n, int mode, int rank, float lam, int batch, ll
   op.gram_mode = 0;
   op.err = nullptr;
   float2* vwide = nullptr;
-  if (n > 64 && n <= kProxMaxN) {   // eigenvector scratch of the wide Jacobi kernel
+  if ((n > 64 && n <= kProxMaxN) || prox_needs_wide_fallback(m, n)) {   // wide Jacobi kernel scratch
     op.vwide_ctas = wide_jacobi_ctas();
     e = cudaMallocAsync((void**)&vwide, sizeof(float2) * (size_t)op.vwide_ctas * (size_t)wide_v_stride(), s);
     if (e != cudaSuccess) {

@@ -87,6 +87,7 @@ int launch_llr_eig_warp(const ProxOp& op, long long nblocks, cudaStream_t stream
 
 int launch_llr_prox(const BlockSource& src, const ProxOp& op, cudaStream_t stream);
 bool llr_prox_supported(int m, int n);
+bool prox_needs_wide_fallback(int m, int n);   // n <= 64 whose blocks the Jacobi kernel cannot stage
 bool llr_gram_tc_supported(int m, int n);
 int launch_llr_gram_tc(const BlockSource& src, const ProxOp& op, cudaStream_t stream);
 

@@ -1169,6 +1169,8 @@ int wide_jacobi_ctas() {
   return nsm;
 }
 
+bool prox_needs_wide_fallback(int m, int n) { return n >= 1 && n <= 64 && !llr_prox_jacobi_supported(m, n); }
+
 bool llr_prox_supported(int m, int n) {
   if (n > 64 && n <= kProxMaxN && m >= 1 && m <= 65535) return make_wide_layout(m, n).total <= 227 * 1024;
   if (m < 1 || n < 1 || n > 64 || m > 65535) return false;
@@ -1176,7 +1178,9 @@ bool llr_prox_supported(int m, int n) {
   if (n <= 16) t = make_trd_layout<16, 2>(m, n).total;
   else if (n <= 32) t = make_trd_layout<32, 2>(m, n).total;
   else t = make_trd_layout<64, 4>(m, n).total;
-  return t <= 227 * 1024 && llr_prox_jacobi_supported(m, n);
+  // the blocks the tridiagonal path hands back go to the Jacobi kernel when a whole block fits in
+  // shared memory, else to the wide kernel, which streams row chunks
+  return t <= 227 * 1024 && (llr_prox_jacobi_supported(m, n) || make_wide_layout(m, n).total <= 227 * 1024);
 }
 
 // Tridiagonal-path prox over every block, then the Jacobi kernel over the blocks it handed
@@ -1216,6 +1220,12 @@ int launch_llr_prox(const BlockSource& src, const ProxOp& op, cudaStream_t strea
   BlockSource fb = src;
   fb.blk_list = op.fb_list;
   fb.blk_count = op.fb_count;
+  if (prox_needs_wide_fallback(op.m, op.n)) {   // a whole block does not fit the Jacobi kernel
+    if (!op.vwide)
+      return set_error(LLR_ERR_UNSUPPORTED, "Casorati %d x %d needs the wide-kernel scratch of a context or of an "
+                                            "allocating entry point for its fallback blocks", op.m, op.n);
+    return launch_prox_wide(fb, op, stream);
+  }
   return launch_llr_prox_jacobi(fb, op, stream);
 }
 
