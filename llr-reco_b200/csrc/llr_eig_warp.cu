@@ -11,10 +11,7 @@
 // different cost (all-zero, certified-zero, full eigen path) never wait on each other:
 //   (tau = (1 - margin) lambda^2 below; eigenvalues between tau and lambda^2 are near threshold)
 //   * soft threshold, ||G||_F <= tau: every eigenvalue is clear below the threshold -> r_a = 0;
-//   * soft threshold, max_i G_ii > tau or the trace lower bound m + s / sqrt(n - 1) > tau
-//     (m = tr G / n, s^2 = ||G||_F^2 / n - m^2, Wolkowicz & Styan 1980): the top eigenvalue is
-//     kept or near -> eigen path;
-//   * the trace upper bound m + s sqrt(n - 1) <= tau: r_a = 0;
+//   * soft threshold, max_i G_ii > tau: the top eigenvalue is kept or near -> eigen path;
 //   * otherwise a Cholesky factorisation of tau I - G certifies r_a = 0 when it succeeds
 //     (every pivot positive) and sends the block to the eigen path when it fails;
 //   * eigen path: Householder tridiagonalisation, unitary diagonal to a real tridiagonal T',
@@ -108,27 +105,13 @@ __device__ bool warp_below(WarpEig<NPMAX>* W, int n, float thr) {
     __syncwarp();
     const int rb1 = rp.i1 >= 0 ? pk(o + rp.i1, o) : 0, rb2 = rp.i2 >= 0 ? pk(o + rp.i2, o) : 0;
     const float2 nl1 = make_float2(-l1.x, -l1.y), nl2 = make_float2(-l2.x, -l2.y);
-    // element s of the lane: row i1 column s for s < n1, else row i2 column s - n1; every
-    // element has one owner lane, so a group's eight loads all go out before its stores
-    const int smax = max(rp.tot - 1, 0);
-    for (int s0 = 0; s0 < rp.tot; s0 += 8) {
-      float2 a[8], uj[8];
-      int id[8];
-#pragma unroll
-      for (int e = 0; e < 8; ++e) {
-        const int sc = min(s0 + e, smax);
-        const bool f = sc < rp.n1;
-        const int j = f ? sc : sc - rp.n1;
-        id[e] = f ? rb1 + sc : rb2 + j;
-        a[e] = A[id[e]];
-        uj[e] = W->u[j];
-      }
-#pragma unroll
-      for (int e = 0; e < 8; ++e) {
-        float2 r = a[e];
-        cfma_cb(r, s0 + e < rp.n1 ? nl1 : nl2, uj[e]);
-        if (s0 + e < rp.tot) A[id[e]] = r;
-      }
+    float2 cl = nl1;
+    int jo = 0, ib = rb1;
+    for (int t = 0; t < rp.tot; ++t) {
+      if (t == rp.n1) { cl = nl2; jo = rp.n1; ib = rb2 - rp.n1; }
+      float2 a = A[ib + t];
+      cfma_cb(a, cl, W->u[t - jo]);
+      A[ib + t] = a;
     }
     __syncwarp();
   }
@@ -168,14 +151,14 @@ __device__ void warp_tridiag(WarpEig<NPMAX>* W, int n) {
     if (rp.i2 >= 0) W->u[rp.i2] = x2;
     __syncwarp();
     // p = t A22 u, reading A22[i][j] = conj(A22[j][i]) above the diagonal.  Lanes without a
-    // row read row 0 (a valid element) and drop the result; eight columns are in flight at once.
+    // row read row 0 (a valid element) and drop the result; four columns are in flight at once.
     const int r1 = max(rp.i1, 0), r2 = max(rp.i2, 0);
     const int rb1 = pk(o + r1, o), rb2 = pk(o + r2, o);
     float2 p1 = z, p2 = z, q1 = z, q2 = z;
-    for (int j0 = 0; j0 < L; j0 += 8) {
-      float2 a1[8], a2[8], uj[8];
+    for (int j0 = 0; j0 < L; j0 += 4) {
+      float2 a1[4], a2[4], uj[4];
 #pragma unroll
-      for (int e = 0; e < 8; ++e) {
+      for (int e = 0; e < 4; ++e) {
         const int j = min(j0 + e, L - 1);
         const int cb = pk(o + j, o);              // trailing row j
         uj[e] = W->u[j];
@@ -183,7 +166,7 @@ __device__ void warp_tridiag(WarpEig<NPMAX>* W, int n) {
         a2[e] = A[j <= r2 ? rb2 + j : cb + r2];
       }
 #pragma unroll
-      for (int e = 0; e < 8; ++e) {
+      for (int e = 0; e < 4; ++e) {
         const int j = j0 + e;
         if (j < L) {                              // warp-uniform
           float2 b1 = a1[e], b2 = a2[e];
@@ -204,15 +187,15 @@ __device__ void warp_tridiag(WarpEig<NPMAX>* W, int n) {
     __syncwarp();
     // A22 -= u w^H + w u^H on the lower triangle of the lane's rows: element s of the lane is
     // row i1 column s for s < n1, else row i2 column s - n1; every element has one owner lane,
-    // so the eight loads of a group can all go out before its stores.
+    // so the four loads of a group can all go out before its stores.
     const float2 nu1 = make_float2(-x1.x, -x1.y), nu2 = make_float2(-x2.x, -x2.y);
     const float2 nw1 = make_float2(-w1.x, -w1.y), nw2 = make_float2(-w2.x, -w2.y);
     const int smax = max(rp.tot - 1, 0);
-    for (int s0 = 0; s0 <= L; s0 += 8) {
-      float2 a[8], wj[8], uj[8];
-      int id[8];
+    for (int s0 = 0; s0 <= L; s0 += 4) {
+      float2 a[4], wj[4], uj[4];
+      int id[4];
 #pragma unroll
-      for (int e = 0; e < 8; ++e) {
+      for (int e = 0; e < 4; ++e) {
         const int sc = min(s0 + e, smax);
         const bool f = sc < rp.n1;
         const int j = f ? sc : sc - rp.n1;
@@ -222,7 +205,7 @@ __device__ void warp_tridiag(WarpEig<NPMAX>* W, int n) {
         uj[e] = W->u[j];
       }
 #pragma unroll
-      for (int e = 0; e < 8; ++e) {
+      for (int e = 0; e < 4; ++e) {
         const bool f = s0 + e < rp.n1;
         float2 r = a[e];
         cfma_cb(r, f ? nu1 : nu2, wj[e]);
@@ -506,25 +489,14 @@ __global__ void __launch_bounds__(32 * kEigWarps, 5) llr_eig_warp_kernel(ProxOp 
       s_all += cabs2(v);
     }
     __syncwarp();
-    float s_diag = 0.f, s_tr = 0.f, dmax = 0.f;
+    float s_diag = 0.f, dmax = 0.f;
     for (int i = lane; i < n; i += 32) {
       const float2 v = W->A[pk(i, i)];
       s_diag += v.x * v.x;
-      s_tr += v.x;
       dmax = fmaxf(dmax, v.x);
     }
     const float fro2 = 2.f * wsum(s_all) - wsum(s_diag);   // ||G||_F^2 from the lower triangle
     dmax = wmax(dmax);
-    // trace bounds on the largest eigenvalue (Wolkowicz & Styan 1980): with m = tr G / n and
-    // s^2 = ||G||_F^2 / n - m^2,  m + s / sqrt(n - 1) <= lambda_max <= m + s sqrt(n - 1)
-    double wub = 0.0, wlb = 0.0;
-    {
-      const double mu = (double)wsum(s_tr) / n;
-      const double sd = sqrt(fmax((double)fro2 / n - mu * mu, 0.0));
-      const double r = n > 1 ? sqrt((double)(n - 1)) : 1.0;
-      wub = mu + sd * r;
-      wlb = mu + sd / r;
-    }
     int ra;
     if (!soft && op.rank >= n) {
       ra = -2;                                            // identity: leave the block as is
@@ -533,11 +505,8 @@ __global__ void __launch_bounds__(32 * kEigWarps, 5) llr_eig_warp_kernel(ProxOp 
     } else if (soft && fro2 <= thr_lo * thr_lo) {
       ra = 0;                                             // lambda_max <= ||G||_F, clear of the margin
     } else {
-      // lambda_max >= max_i G_ii and >= the trace lower bound: a kept or near component
-      bool eig = !soft || dmax > thr_lo || wlb > (double)thr_lo;
-      if (!eig && wub <= (double)thr_lo) {
-        // the trace upper bound certifies every eigenvalue below the threshold: r_a = 0
-      } else if (!eig) {
+      bool eig = !soft || dmax > thr_lo;                  // lambda_max >= max_i G_ii
+      if (!eig) {
         eig = !warp_below(W, n, thr_lo);
         if (eig) {                                        // the test overwrote A: reload
           for (int i = lane; i < P; i += 32) W->A[i] = G[i];
