@@ -1057,6 +1057,27 @@ __global__ void __launch_bounds__(kLlrThreads, 1) llr_prox_wide_kernel(BlockSour
     for (int k = tid; k < ((n + 1) & ~1) * lda; k += blockDim.x) A[k] = make_float2(0.f, 0.f);
     gram_block<NP, kWideTG>(src, W.t, m, n, blk, base, qstride, sh, rows, rowph, Cch,
                             [&](int a, int b, float2 v) { A[a * lda + b] = v; });
+    if (!op.block_stat && op.mode != LLR_PROX_HARD_RANK && op.lambda > 0.f) {
+      // ||G||_F <= lambda^2 bounds every eigenvalue of G = C^H C below the threshold: the output
+      // is zero, as the Jacobi path would make it (no kept component, W = 0), without the sweeps
+      __syncthreads();
+      float loc = 0.f;
+      for (int k = tid; k < n * n; k += blockDim.x) {
+        const int a = k / n, b = k - a * n;
+        loc += cabs2(A[a * lda + b]);
+      }
+      const float fro2 = block_sum(loc, misc->red);
+      const float thr = op.lambda * op.lambda;
+      if (fro2 <= thr * thr) {
+        if (!src.accumulate)
+          for (int e = tid; e < m * n; e += blockDim.x) {
+            const int q = e / m, r = e - q * m;
+            store_elem(src, base, rows[r], rowph, r, q, qstride, make_float2(0.f, 0.f));
+          }
+        __syncthreads();
+        continue;
+      }
+    }
     jacobi<NP>(A, V, n, rot, pairs, misc, 20, lda);
     if (op.block_stat) {
       if (tid == 0) {
