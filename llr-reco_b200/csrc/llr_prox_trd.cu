@@ -1058,17 +1058,23 @@ __global__ void __launch_bounds__(kLlrThreads, 1) llr_prox_wide_kernel(BlockSour
     gram_block<NP, kWideTG>(src, W.t, m, n, blk, base, qstride, sh, rows, rowph, Cch,
                             [&](int a, int b, float2 v) { A[a * lda + b] = v; });
     if (!op.block_stat && op.mode != LLR_PROX_HARD_RANK && op.lambda > 0.f) {
-      // ||G||_F <= lambda^2 bounds every eigenvalue of G = C^H C below the threshold: the output
-      // is zero, as the Jacobi path would make it (no kept component, W = 0), without the sweeps
+      // ||G||_F <= lambda^2, or the trace bound lambda_max <= m + s sqrt(n - 1) (m = tr G / n,
+      // s^2 = ||G||_F^2 / n - m^2; Wolkowicz & Styan 1980) <= lambda^2, puts every eigenvalue of
+      // G = C^H C below the threshold: the output is zero, as the Jacobi path would make it (no kept
+      // component, W = 0), without the sweeps
       __syncthreads();
-      float loc = 0.f;
+      float loc = 0.f, tr = 0.f;
       for (int k = tid; k < n * n; k += blockDim.x) {
         const int a = k / n, b = k - a * n;
         loc += cabs2(A[a * lda + b]);
+        if (a == b) tr += A[a * lda + b].x;
       }
       const float fro2 = block_sum(loc, misc->red);
+      const float trace = block_sum(tr, misc->red);
       const float thr = op.lambda * op.lambda;
-      if (fro2 <= thr * thr) {
+      const double mu = (double)trace / n;
+      const double ub = mu + sqrt(fmax((double)fro2 / n - mu * mu, 0.0)) * sqrt((double)(n > 1 ? n - 1 : 1));
+      if (fro2 <= thr * thr || ub <= (double)thr) {
         if (!src.accumulate)
           for (int e = tid; e < m * n; e += blockDim.x) {
             const int q = e / m, r = e - q * m;
