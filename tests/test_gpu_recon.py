@@ -186,13 +186,16 @@ def test_fused_fft_dc(gpu, vol, fft_mode):
     check(gx, ox, gh, oh)
 
 
-def test_fused_fft_dc_c2_plane(gpu):
+@pytest.mark.parametrize("nx,nq", [(6, 5), (48, 7)])
+def test_fused_fft_dc_c2_plane(gpu, nx, nq):
     """The 192 x 96 (y, z) plane of the production configuration (16 x 12 and 12 x 8 register
-    DFTs), fused against cuFFT on the same data."""
-    d = dataset((6, 192, 96), 5, accel=8.0, centre=8)
+    DFTs), fused against cuFFT on the same data.  6 x 5 planes: one plane per CTA; 48 x 7 = 336
+    planes: every CTA transforms several, so the next plane's rows are staged while the current
+    one is transformed."""
+    d = dataset((nx, 192, 96), nq, accel=8.0, centre=8)
     out = {}
     for mode in (0, 1):
-        p = ReconParams(vol_size=(6, 192, 96), nq=5, block_size=(6, 6, 6), prox_mode=L.LLR_PROX_SOFT_THRESH,
+        p = ReconParams(vol_size=(nx, 192, 96), nq=nq, block_size=(6, 6, 6), prox_mode=L.LLR_PROX_SOFT_THRESH,
                         lam=0.5, seed=3, fft_mode=mode)
         with ReconContext(p) as ctx:
             ctx.upload_kspace(d.y)
