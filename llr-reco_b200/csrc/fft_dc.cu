@@ -285,8 +285,43 @@ __device__ __forceinline__ void axis_pass_fixed(float2* s, const float2* wN) {
   }
 }
 
+// First forward / last inverse pass of the z axis (step 0: DFTs of length Z1 at stride Z2 down z)
+// on the plane in HBM (element (y, z) at g[y + ny z], lanes along y: 256-byte warp accesses) and
+// the shared plane (row pitch PP) on the other side: the forward pass loads its elements straight
+// into registers, zero-filling those of zero blocks (zero(y, z)), and stores the twiddled result
+// in shared memory; the inverse pass reads shared memory and stores its result to HBM.
+template <int DIR, int NY, int PP, int Z1, int Z2, int NT, class ZeroFn>
+__device__ __forceinline__ void z_pass_hbm(float2* s, float2* g, const float2* wN, ZeroFn zero) {
+  constexpr int TASKS = NY * Z2;
+#pragma unroll 1
+  for (int t = threadIdx.x; t < TASKS; t += NT) {
+    const int y = t % NY, j = t / NY;
+    float2* sb = s + y + PP * j;
+    float2* gb = g + y + NY * j;
+    float2 v[Z1];
+    if (DIR > 0) {
+#pragma unroll
+      for (int i = 0; i < Z1; ++i) v[i] = zero(y, Z2 * i + j) ? make_float2(0.f, 0.f) : gb[NY * Z2 * i];
+      Dft<Z1, DIR>::run(v, nullptr);
+#pragma unroll
+      for (int i = 1; i < Z1; ++i) v[i] = twmul<DIR>(v[i], wN[j * i]);
+#pragma unroll
+      for (int i = 0; i < Z1; ++i) sb[PP * Z2 * i] = v[i];
+    } else {
+#pragma unroll
+      for (int i = 0; i < Z1; ++i) v[i] = sb[PP * Z2 * i];
+#pragma unroll
+      for (int i = 1; i < Z1; ++i) v[i] = twmul<DIR>(v[i], wN[j * i]);
+      Dft<Z1, DIR>::run(v, nullptr);
+#pragma unroll
+      for (int i = 0; i < Z1; ++i) gb[NY * Z2 * i] = v[i];
+    }
+  }
+}
+
 // Plane geometry with run-time sizes (any shape split_len accepts).
 struct GeoRt {
+  static constexpr bool kHbmPasses = false;
   int ny, nz, y1, y2, z1, z2, P;
   __device__ void forward(float2* s, const float2* tw, const FftTab& T) const {
     axis_dispatch<1, 0>(s, nz, P, 1, y1, y2, tw + T.off_y, ny, tw, T);
@@ -308,28 +343,34 @@ struct GeoRt {
   }
 };
 
-// Plane geometry with compile-time sizes: ny = Y1 Y2, nz = Z1 Z2, NT threads.
+// Plane geometry with compile-time sizes: ny = Y1 Y2, nz = Z1 Z2, NT threads.  The forward
+// transform runs the z axis first and the inverse the z axis last, so that the z axis's step-0
+// pass reads (forward) and writes (inverse) the plane in HBM directly; the y-axis passes and the
+// z axis's step 1 run in shared memory.  Each axis leaves its spectrum in the same permuted order
+// whichever axis runs first.
 template <int Y1, int Y2, int Z1, int Z2, int NT>
 struct GeoFixed {
+  static constexpr bool kHbmPasses = true;
   static constexpr int NY = Y1 * Y2, NZ = Z1 * Z2, PP = NY | 1;
   int ny = NY, nz = NZ, y1 = Y1, y2 = Y2, z1 = Z1, z2 = Z2, P = PP;
-  __device__ void forward(float2* s, const float2* tw, const FftTab& T) const {
+  template <class ZeroFn>
+  __device__ void forward_hbm(float2* s, float2* g, const float2* tw, const FftTab& T, ZeroFn zero) const {
+    z_pass_hbm<1, NY, PP, Z1, Z2, NT>(s, g, tw + T.off_z, zero);
+    __syncthreads();
+    axis_pass_fixed<1, 1, NY, 1, PP, Z1, Z2, NT>(s, tw + T.off_z);
+    __syncthreads();
     axis_pass_fixed<1, 0, NZ, PP, 1, Y1, Y2, NT>(s, tw + T.off_y);
     __syncthreads();
     axis_pass_fixed<1, 1, NZ, PP, 1, Y1, Y2, NT>(s, tw + T.off_y);
-    __syncthreads();
-    axis_pass_fixed<1, 0, NY, 1, PP, Z1, Z2, NT>(s, tw + T.off_z);
-    __syncthreads();
-    axis_pass_fixed<1, 1, NY, 1, PP, Z1, Z2, NT>(s, tw + T.off_z);
   }
-  __device__ void inverse(float2* s, const float2* tw, const FftTab& T) const {
-    axis_pass_fixed<-1, 1, NY, 1, PP, Z1, Z2, NT>(s, tw + T.off_z);
-    __syncthreads();
-    axis_pass_fixed<-1, 0, NY, 1, PP, Z1, Z2, NT>(s, tw + T.off_z);
-    __syncthreads();
+  __device__ void inverse_hbm(float2* s, float2* g, const float2* tw, const FftTab& T) const {
     axis_pass_fixed<-1, 1, NZ, PP, 1, Y1, Y2, NT>(s, tw + T.off_y);
     __syncthreads();
     axis_pass_fixed<-1, 0, NZ, PP, 1, Y1, Y2, NT>(s, tw + T.off_y);
+    __syncthreads();
+    axis_pass_fixed<-1, 1, NY, 1, PP, Z1, Z2, NT>(s, tw + T.off_z);
+    __syncthreads();
+    z_pass_hbm<-1, NY, PP, Z1, Z2, NT>(s, g, tw + T.off_z, [](int, int) { return false; });
   }
 };
 
@@ -395,23 +436,28 @@ __device__ __forceinline__ void fft_dc_body(const FftDcArgs& a, const Geo& geo) 
         zfl[t] = gxi >= 0 && a.zero_ra[t + (long long)nslab * gxi] == 0;
       __syncthreads();
     }
-    {   // asynchronous 8-byte copies: every element in flight at once, no register staging
-      int z = tid / ny, y = tid - (tid / ny) * ny;
-      for (int e = tid; e < ny * nz; e += blockDim.x) {
-        const unsigned dst = (unsigned)__cvta_generic_to_shared(s + z * P + y);
-        if (zero_at(y, z))
-          s[z * P + y] = make_float2(0.f, 0.f);
-        else
-          asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(g + e) : "memory");
-        y += dy;
-        z += dz;
-        if (y >= ny) { y -= ny; ++z; }
+    if constexpr (Geo::kHbmPasses) {
+      // forward: z axis (its first pass loads the plane from HBM), then y axis
+      geo.forward_hbm(s, g, tw, T, zero_at);
+    } else {
+      {   // asynchronous 8-byte copies: every element in flight at once, no register staging
+        int z = tid / ny, y = tid - (tid / ny) * ny;
+        for (int e = tid; e < ny * nz; e += blockDim.x) {
+          const unsigned dst = (unsigned)__cvta_generic_to_shared(s + z * P + y);
+          if (zero_at(y, z))
+            s[z * P + y] = make_float2(0.f, 0.f);
+          else
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(g + e) : "memory");
+          y += dy;
+          z += dz;
+          if (y >= ny) { y -= ny; ++z; }
+        }
+        asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
       }
-      asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
+      __syncthreads();
+      // forward: y axis (rows, element stride 1, batch stride P), then z axis (columns)
+      geo.forward(s, tw, T);
     }
-    __syncthreads();
-    // forward: y axis (rows, element stride 1, batch stride P), then z axis (columns)
-    geo.forward(s, tw, T);
     __syncthreads();
     // hard DC on the sampled lines of this plane
     {
@@ -430,10 +476,13 @@ __device__ __forceinline__ void fft_dc_body(const FftDcArgs& a, const Geo& geo) 
       }
     }
     __syncthreads();
-    // inverse: z axis then y axis, each mirrored (step 1 then step 0)
-    geo.inverse(s, tw, T);
-    __syncthreads();
-    {
+    if constexpr (Geo::kHbmPasses) {
+      // inverse: y axis, then z axis (its last pass stores the plane to HBM)
+      geo.inverse_hbm(s, g, tw, T);
+    } else {
+      // inverse: z axis then y axis, each mirrored (step 1 then step 0)
+      geo.inverse(s, tw, T);
+      __syncthreads();
       int z = tid / ny, y = tid - (tid / ny) * ny;
       for (int e = tid; e < ny * nz; e += blockDim.x) {
         g[e] = s[z * P + y];
